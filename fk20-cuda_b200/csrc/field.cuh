@@ -1,0 +1,309 @@
+// field.cuh -- BLS12-381 Fp (381-bit) and Fr (255-bit) Montgomery arithmetic.
+//
+// Elements are little-endian arrays of 32-bit limbs (Fp: 12, Fr: 8).  Inside
+// the engine Fp values are in Montgomery form (x*2^384 mod p) and always
+// canonical (< p); Fr data keeps its standard form and is multiplied by
+// Montgomery-form constants (x*y*2^-256 with y = w*2^256 gives x*w), so Fr
+// FFT outputs are standard-form without conversions.  The reference stores
+// plain (non-Montgomery) values with Barrett reduction (fp.cuh:10-14,
+// fr.cuh:10-24, fr_mul.cu:58-186); conversion happens at the ABI boundary.
+//
+// Montgomery product: word-serial CIOS with the partial products of each
+// word b_i split between two accumulators, `e` (products a_j*b_i with j even:
+// lo at word j, hi at word j+1) and `o` (j odd).  Within one accumulator the
+// lo/hi words of different j never overlap, so each half is a single
+// mad.lo.cc/madc.hi.cc carry chain and the two chains are independent.  The
+// reduction multiple m*p is split the same way.  After the reduction the
+// word-0 sum e0+o0 is 0 mod 2^32; its carry (0 or 1) is fed into the next
+// iteration at word 0 of the odd chain, and both accumulators shift down one
+// word.  Bounds: with inputs < 2p and 4p < 2^384 every partial value stays
+// below 2^416, so 13 words per accumulator suffice and the final value is
+// < 2p (one conditional subtraction of p makes it canonical).
+#pragma once
+#include "limbs.cuh"
+
+namespace fk {
+
+// ---------------------------------------------------------------- moduli
+struct FpDesc {
+    static constexpr int N = 12;
+    static constexpr uint32_t M0 = 0xfffcfffdu;  // -p^-1 mod 2^32
+    FK_HD static constexpr uint32_t mod(int i) {
+        return i == 0 ? 0xffffaaabu : i == 1 ? 0xb9feffffu : i == 2 ? 0xb153ffffu : i == 3 ? 0x1eabfffeu
+             : i == 4 ? 0xf6b0f624u : i == 5 ? 0x6730d2a0u : i == 6 ? 0xf38512bfu : i == 7 ? 0x64774b84u
+             : i == 8 ? 0x434bacd7u : i == 9 ? 0x4b1ba7b6u : i == 10 ? 0x397fe69au : 0x1a0111eau;
+    }
+    // 2^768 mod p (to Montgomery form)
+    FK_HD static constexpr uint32_t r2(int i) {
+        return i == 0 ? 0x1c341746u : i == 1 ? 0xf4df1f34u : i == 2 ? 0x09d104f1u : i == 3 ? 0x0a76e6a6u
+             : i == 4 ? 0x4c95b6d5u : i == 5 ? 0x8de5476cu : i == 6 ? 0x939d83c0u : i == 7 ? 0x67eb88a9u
+             : i == 8 ? 0xb519952du : i == 9 ? 0x9a793e85u : i == 10 ? 0x92cae3aau : 0x11988fe5u;
+    }
+    // 2^384 mod p (Montgomery one)
+    FK_HD static constexpr uint32_t one(int i) {
+        return i == 0 ? 0x0002fffdu : i == 1 ? 0x76090000u : i == 2 ? 0xc40c0002u : i == 3 ? 0xebf4000bu
+             : i == 4 ? 0x53c758bau : i == 5 ? 0x5f489857u : i == 6 ? 0x70525745u : i == 7 ? 0x77ce5853u
+             : i == 8 ? 0xa256ec6du : i == 9 ? 0x5c071a97u : i == 10 ? 0xfa80e493u : 0x15f65ec3u;
+    }
+};
+
+struct FrDesc {
+    static constexpr int N = 8;
+    static constexpr uint32_t M0 = 0xffffffffu;  // -r^-1 mod 2^32
+    FK_HD static constexpr uint32_t mod(int i) {
+        return i == 0 ? 0x00000001u : i == 1 ? 0xffffffffu : i == 2 ? 0xfffe5bfeu : i == 3 ? 0x53bda402u
+             : i == 4 ? 0x09a1d805u : i == 5 ? 0x3339d808u : i == 6 ? 0x299d7d48u : 0x73eda753u;
+    }
+    FK_HD static constexpr uint32_t r2(int i) {
+        return i == 0 ? 0xf3f29c6du : i == 1 ? 0xc999e990u : i == 2 ? 0x87925c23u : i == 3 ? 0x2b6cedcbu
+             : i == 4 ? 0x7254398fu : i == 5 ? 0x05d31496u : i == 6 ? 0x9f59ff11u : 0x0748d9d9u;
+    }
+    FK_HD static constexpr uint32_t one(int i) {
+        return i == 0 ? 0xfffffffeu : i == 1 ? 0x00000001u : i == 2 ? 0x00034802u : i == 3 ? 0x5884b7fau
+             : i == 4 ? 0xecbc4ff5u : i == 5 ? 0x998c4fefu : i == 6 ? 0xacc5056fu : 0x1824b159u;
+    }
+};
+
+template <class F>
+struct Elem {
+    uint32_t w[F::N];
+};
+using Fp = Elem<FpDesc>;
+using Fr = Elem<FrDesc>;
+
+// ---------------------------------------------------------------- helpers
+template <class F>
+FK_HD void f_set_zero(Elem<F> &r) {
+#pragma unroll
+    for (int i = 0; i < F::N; i++) r.w[i] = 0;
+}
+
+template <class F>
+FK_HD void f_set_one(Elem<F> &r) {  // Montgomery one
+#pragma unroll
+    for (int i = 0; i < F::N; i++) r.w[i] = F::one(i);
+}
+
+template <class F>
+FK_HD bool f_is_zero(const Elem<F> &a) {
+    uint32_t o = 0;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) o |= a.w[i];
+    return o == 0;
+}
+
+template <class F>
+FK_HD bool f_eq(const Elem<F> &a, const Elem<F> &b) {
+    uint32_t o = 0;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) o |= a.w[i] ^ b.w[i];
+    return o == 0;
+}
+
+// r = t - mod if t >= mod else t   (t < 2*mod < 2^(32N))
+template <class F>
+FK_HD void f_reduce_once(uint32_t r[F::N], const uint32_t t[F::N]) {
+    constexpr int N = F::N;
+    uint32_t s[N];
+    s[0] = sub_cc(t[0], F::mod(0));
+#pragma unroll
+    for (int i = 1; i < N; i++) s[i] = subc_cc(t[i], F::mod(i));
+    uint32_t borrow = subc(0u, 0u);  // 0xffffffff if t < mod
+#pragma unroll
+    for (int i = 0; i < N; i++) r[i] = (t[i] & borrow) | (s[i] & ~borrow);
+}
+
+// ---------------------------------------------------------------- Montgomery product
+template <class F>
+FK_HD void f_mul(Elem<F> &r, const Elem<F> &A, const Elem<F> &B) {
+    constexpr int N = F::N;
+    const uint32_t *a = A.w;
+    uint32_t e[N + 1], o[N + 1];
+    uint32_t c = 0;
+
+    // word 0 of b: plain products, no chains needed
+    {
+        const uint32_t bi = B.w[0];
+#pragma unroll
+        for (int j = 0; j < N; j += 2) {
+            e[j] = mul_lo(a[j], bi);
+            e[j + 1] = mul_hi(a[j], bi);
+        }
+        e[N] = 0;
+        o[0] = 0;
+#pragma unroll
+        for (int j = 1; j < N; j += 2) {
+            o[j] = mul_lo(a[j], bi);
+            o[j + 1] = mul_hi(a[j], bi);
+        }
+    }
+
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        if (i > 0) {
+            const uint32_t bi = B.w[i];
+            // even products into e[0..N]
+            e[0] = mad_lo_cc(a[0], bi, e[0]);
+            e[1] = madc_hi_cc(a[0], bi, e[1]);
+#pragma unroll
+            for (int j = 2; j < N; j += 2) {
+                e[j] = madc_lo_cc(a[j], bi, e[j]);
+                e[j + 1] = madc_hi_cc(a[j], bi, e[j + 1]);
+            }
+            e[N] = addc(0u, 0u);
+            // carry of the previous word-0 sum, then odd products into o[0..N]
+            o[0] = add_cc(o[0], c);
+#pragma unroll
+            for (int j = 1; j < N - 1; j += 2) {
+                o[j] = madc_lo_cc(a[j], bi, o[j]);
+                o[j + 1] = madc_hi_cc(a[j], bi, o[j + 1]);
+            }
+            o[N - 1] = madc_lo_cc(a[N - 1], bi, o[N - 1]);
+            o[N] = madc_hi(a[N - 1], bi, 0u);
+        }
+        // reduction: add m*p, m chosen so that word 0 vanishes
+        const uint32_t m = mul_lo(e[0] + o[0], F::M0);
+        e[0] = mad_lo_cc(m, F::mod(0), e[0]);
+        e[1] = madc_hi_cc(m, F::mod(0), e[1]);
+#pragma unroll
+        for (int j = 2; j < N; j += 2) {
+            e[j] = madc_lo_cc(m, F::mod(j), e[j]);
+            e[j + 1] = madc_hi_cc(m, F::mod(j), e[j + 1]);
+        }
+        e[N] = addc(e[N], 0u);
+        o[1] = mad_lo_cc(m, F::mod(1), o[1]);
+        o[2] = madc_hi_cc(m, F::mod(1), o[2]);
+#pragma unroll
+        for (int j = 3; j < N - 1; j += 2) {
+            o[j] = madc_lo_cc(m, F::mod(j), o[j]);
+            o[j + 1] = madc_hi_cc(m, F::mod(j), o[j + 1]);
+        }
+        o[N - 1] = madc_lo_cc(m, F::mod(N - 1), o[N - 1]);
+        o[N] = madc_hi(m, F::mod(N - 1), o[N]);
+
+        if (i < N - 1) {
+            (void)add_cc(e[0], o[0]);
+            c = addc(0u, 0u);
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                e[k] = e[k + 1];
+                o[k] = o[k + 1];
+            }
+            e[N] = 0;
+            o[N] = 0;
+        }
+    }
+    // final: (e + o) >> 32, then one conditional subtraction
+    uint32_t t[N];
+    (void)add_cc(e[0], o[0]);
+#pragma unroll
+    for (int k = 1; k < N; k++) t[k - 1] = addc_cc(e[k], o[k]);
+    t[N - 1] = addc(e[N], o[N]);
+    f_reduce_once<F>(r.w, t);
+}
+
+template <class F>
+FK_HD void f_sqr(Elem<F> &r, const Elem<F> &a) { f_mul<F>(r, a, a); }
+
+template <class F>
+FK_HD void f_add(Elem<F> &r, const Elem<F> &a, const Elem<F> &b) {
+    constexpr int N = F::N;
+    uint32_t t[N];
+    t[0] = add_cc(a.w[0], b.w[0]);
+#pragma unroll
+    for (int i = 1; i < N - 1; i++) t[i] = addc_cc(a.w[i], b.w[i]);
+    t[N - 1] = addc(a.w[N - 1], b.w[N - 1]);
+    f_reduce_once<F>(r.w, t);
+}
+
+template <class F>
+FK_HD void f_sub(Elem<F> &r, const Elem<F> &a, const Elem<F> &b) {
+    constexpr int N = F::N;
+    uint32_t t[N];
+    t[0] = sub_cc(a.w[0], b.w[0]);
+#pragma unroll
+    for (int i = 1; i < N; i++) t[i] = subc_cc(a.w[i], b.w[i]);
+    uint32_t borrow = subc(0u, 0u);
+    r.w[0] = add_cc(t[0], F::mod(0) & borrow);
+#pragma unroll
+    for (int i = 1; i < N - 1; i++) r.w[i] = addc_cc(t[i], F::mod(i) & borrow);
+    r.w[N - 1] = addc(t[N - 1], F::mod(N - 1) & borrow);
+}
+
+template <class F>
+FK_HD void f_neg(Elem<F> &r, const Elem<F> &a) {
+    Elem<F> z;
+    f_set_zero(z);
+    f_sub<F>(r, z, a);
+}
+
+template <class F>
+FK_HD void f_dbl(Elem<F> &r, const Elem<F> &a) { f_add<F>(r, a, a); }
+
+// r = 12 a  (3b for b = 4)
+template <class F>
+FK_HD void f_mul12(Elem<F> &r, const Elem<F> &a) {
+    Elem<F> t;
+    f_add<F>(t, a, a);
+    f_add<F>(t, t, a);
+    f_add<F>(t, t, t);
+    f_add<F>(r, t, t);
+}
+
+template <class F>
+FK_HD void f_cmov(Elem<F> &r, const Elem<F> &a, bool cond) {
+    const uint32_t m = cond ? 0xffffffffu : 0u;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) r.w[i] = (a.w[i] & m) | (r.w[i] & ~m);
+}
+
+// standard form (any value < 2^(32N)) -> Montgomery form, canonical
+template <class F>
+FK_HD void f_to_mont(Elem<F> &r, const Elem<F> &a) {
+    Elem<F> r2;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) r2.w[i] = F::r2(i);
+    f_mul<F>(r, a, r2);
+}
+
+// Montgomery form -> canonical standard form
+template <class F>
+FK_HD void f_from_mont(Elem<F> &r, const Elem<F> &a) {
+    Elem<F> one;
+    f_set_zero(one);
+    one.w[0] = 1;
+    f_mul<F>(r, a, one);
+}
+
+// canonical reduction of any standard-form value < 2^(32N)
+template <class F>
+FK_HD void f_canon(Elem<F> &r, const Elem<F> &a) {
+    Elem<F> t;
+    f_to_mont<F>(t, a);
+    f_from_mont<F>(r, t);
+}
+
+// r = a^e for a little-endian exponent of `nw` 32-bit words (Montgomery domain)
+template <class F>
+FK_HD void f_pow(Elem<F> &r, const Elem<F> &a, const uint32_t *e, int nw) {
+    Elem<F> acc;
+    f_set_one(acc);
+    for (int i = 32 * nw - 1; i >= 0; i--) {
+        f_sqr<F>(acc, acc);
+        if ((e[i >> 5] >> (i & 31)) & 1) f_mul<F>(acc, acc, a);
+    }
+    r = acc;
+}
+
+// inverse by Fermat's little theorem, a^(m-2); inv(0) = 0
+template <class F>
+FK_HD void f_inv(Elem<F> &r, const Elem<F> &a) {
+    uint32_t e[F::N];
+    e[0] = sub_cc(F::mod(0), 2u);
+#pragma unroll
+    for (int i = 1; i < F::N - 1; i++) e[i] = subc_cc(F::mod(i), 0u);
+    e[F::N - 1] = subc(F::mod(F::N - 1), 0u);
+    f_pow<F>(r, a, e, F::N);
+}
+
+}  // namespace fk

@@ -1,0 +1,200 @@
+// g1.cuh -- BLS12-381 G1 (y^2 = x^3 + 4 over Fp) in homogeneous projective
+// coordinates (x = X/Z, y = Y/Z), the reference's convention (g1.cuh:20-29),
+// with the complete addition laws of Renes, Costello and Batina (eprint
+// 2015/1060): Algorithm 7 (addition), 8 (mixed addition) and 9 (doubling) for
+// a = 0, b3 = 3*b = 12.  Complete means no exceptional inputs: P + P, P + (-P)
+// and the point at infinity (0 : Y : 0) all go through the same straight-line
+// code, so warps never diverge on point values.  Coordinates are Montgomery
+// Fp elements (field.cuh).
+#pragma once
+#include "field.cuh"
+
+namespace fk {
+
+struct G1P {
+    Fp x, y, z;
+};
+struct G1A {
+    Fp x, y;
+};
+
+FK_HD void g1_set_inf(G1P &p) {
+    f_set_zero(p.x);
+    f_set_one(p.y);
+    f_set_zero(p.z);
+}
+
+FK_HD bool g1_is_inf(const G1P &p) { return f_is_zero(p.z); }
+
+FK_HD void g1_neg(G1P &r, const G1P &p) {
+    r.x = p.x;
+    f_neg(r.y, p.y);
+    r.z = p.z;
+}
+
+// Q accessor for a point held in registers
+struct RegPoint {
+    const G1P &p;
+    FK_HD void get(int c, Fp &f) const { f = c == 0 ? p.x : c == 1 ? p.y : p.z; }
+};
+
+// Q accessor for a point stored word-strided (word k at base[k * stride]),
+// e.g. one thread's slot in a conflict-free shared-memory array
+struct StridedPoint {
+    uint32_t *base;
+    int stride;
+    FK_HD void get(int c, Fp &f) const {
+#pragma unroll
+        for (int k = 0; k < 12; k++) f.w[k] = base[(12 * c + k) * stride];
+    }
+    FK_HD void put(const G1P &p) const {
+#pragma unroll
+        for (int k = 0; k < 12; k++) {
+            base[k * stride] = p.x.w[k];
+            base[(12 + k) * stride] = p.y.w[k];
+            base[(24 + k) * stride] = p.z.w[k];
+        }
+    }
+    FK_HD void load(G1P &p) const {
+        get(0, p.x);
+        get(1, p.y);
+        get(2, p.z);
+    }
+};
+
+// R = P + (negQ ? -Q : Q), Algorithm 7 with Q read through an accessor as
+// needed (keeps Q out of registers) and the sign folded into the two places
+// Y2 enters: t1 = Y1*Y2 and the sums X2+Y2, Y2+Z2.
+template <class QT>
+FK_HD void g1_add_q(G1P &R, const G1P &P, const QT &Q, bool negQ) {
+    Fp t0, t1, t2, t3, t4, X3, Y3, Z3, q;
+    Q.get(0, q);
+    f_mul(t0, P.x, q);
+    Q.get(1, q);
+    f_mul(t1, P.y, q);
+    if (negQ) f_neg(t1, t1);
+    Q.get(2, q);
+    f_mul(t2, P.z, q);
+    f_add(t3, P.x, P.y);
+    Q.get(0, q);
+    Q.get(1, t4);
+    if (negQ) f_sub(t4, q, t4); else f_add(t4, q, t4);
+    f_mul(t3, t3, t4);
+    f_add(t4, t0, t1);
+    f_sub(t3, t3, t4);
+    f_add(t4, P.y, P.z);
+    Q.get(2, q);
+    Q.get(1, X3);
+    if (negQ) f_sub(X3, q, X3); else f_add(X3, X3, q);
+    f_mul(t4, t4, X3);
+    f_add(X3, t1, t2);
+    f_sub(t4, t4, X3);
+    f_add(X3, P.x, P.z);
+    Q.get(0, q);
+    Q.get(2, Y3);
+    f_add(Y3, q, Y3);
+    f_mul(X3, X3, Y3);
+    f_add(Y3, t0, t2);
+    f_sub(Y3, X3, Y3);
+    f_add(X3, t0, t0);
+    f_add(t0, X3, t0);
+    f_mul12(t2, t2);
+    f_add(Z3, t1, t2);
+    f_sub(t1, t1, t2);
+    f_mul12(Y3, Y3);
+    f_mul(X3, t4, Y3);
+    f_mul(t2, t3, t1);
+    f_sub(X3, t2, X3);
+    f_mul(Y3, Y3, t0);
+    f_mul(t1, t1, Z3);
+    f_add(Y3, t1, Y3);
+    f_mul(t0, t0, t3);
+    f_mul(Z3, Z3, t4);
+    f_add(Z3, Z3, t0);
+    R.x = X3;
+    R.y = Y3;
+    R.z = Z3;
+}
+
+// R = P + Q (RCB Algorithm 7, 12 M + 2 m_3b)
+FK_HD void g1_add(G1P &R, const G1P &P, const G1P &Q) { g1_add_q(R, P, RegPoint{Q}, false); }
+
+// R = P + (qx, qy) with Q affine and not infinity (RCB Algorithm 8, 11 M + 2 m_3b)
+FK_HD void g1_madd(G1P &R, const G1P &P, const Fp &qx, const Fp &qy) {
+    Fp t0, t1, t2, t3, t4, X3, Y3, Z3;
+    f_mul(t0, P.x, qx);
+    f_mul(t1, P.y, qy);
+    f_add(t3, qx, qy);
+    f_add(t4, P.x, P.y);
+    f_mul(t3, t3, t4);
+    f_add(t4, t0, t1);
+    f_sub(t3, t3, t4);
+    f_mul(t4, qy, P.z);
+    f_add(t4, t4, P.y);
+    f_mul(Y3, qx, P.z);
+    f_add(Y3, Y3, P.x);
+    f_add(X3, t0, t0);
+    f_add(t0, X3, t0);
+    f_mul12(t2, P.z);
+    f_add(Z3, t1, t2);
+    f_sub(t1, t1, t2);
+    f_mul12(Y3, Y3);
+    f_mul(X3, t4, Y3);
+    f_mul(t2, t3, t1);
+    f_sub(X3, t2, X3);
+    f_mul(Y3, Y3, t0);
+    f_mul(t1, t1, Z3);
+    f_add(Y3, t1, Y3);
+    f_mul(t0, t0, t3);
+    f_mul(Z3, Z3, t4);
+    f_add(Z3, Z3, t0);
+    R.x = X3;
+    R.y = Y3;
+    R.z = Z3;
+}
+
+// R = 2P (RCB Algorithm 9, 6 M + 2 S + 1 m_3b)
+FK_HD void g1_dbl(G1P &R, const G1P &P) {
+    Fp t0, t1, t2, X3, Y3, Z3;
+    f_sqr(t0, P.y);
+    f_add(Z3, t0, t0);
+    f_add(Z3, Z3, Z3);
+    f_add(Z3, Z3, Z3);
+    f_mul(t1, P.y, P.z);
+    f_sqr(t2, P.z);
+    f_mul12(t2, t2);
+    f_mul(X3, t2, Z3);
+    f_add(Y3, t0, t2);
+    f_mul(Z3, t1, Z3);
+    f_add(t1, t2, t2);
+    f_add(t2, t1, t2);
+    f_sub(t0, t0, t2);
+    f_mul(Y3, t0, Y3);
+    f_add(Y3, X3, Y3);
+    f_mul(t1, P.x, P.y);
+    f_mul(X3, t0, t1);
+    f_add(X3, X3, X3);
+    R.x = X3;
+    R.y = Y3;
+    R.z = Z3;
+}
+
+// GLV endomorphism phi(x, y) = (beta x, y) = [lambda] P on G1, with
+// lambda = z^2 - 1 (z = -0xd201000000010000) and beta the cube root of unity
+// in Fp below (Montgomery form).  r = lambda^2 + lambda + 1.
+FK_HD constexpr uint32_t beta_mont(int i) {
+    return i == 0 ? 0x8671f071u : i == 1 ? 0xcd03c9e4u : i == 2 ? 0x1fcda5d2u : i == 3 ? 0x5dab2246u
+         : i == 4 ? 0xd3851b95u : i == 5 ? 0x587042afu : i == 6 ? 0x01bacb9eu : i == 7 ? 0x8eb60ebeu
+         : i == 8 ? 0x83d050d2u : i == 9 ? 0x03f97d6eu : i == 10 ? 0x54638741u : 0x18f02065u;
+}
+
+FK_HD void g1_phi(G1P &R, const G1P &P) {
+    Fp beta;
+#pragma unroll
+    for (int i = 0; i < 12; i++) beta.w[i] = beta_mont(i);
+    f_mul(R.x, P.x, beta);
+    R.y = P.y;
+    R.z = P.z;
+}
+
+}  // namespace fk

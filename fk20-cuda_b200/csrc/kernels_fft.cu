@@ -1,0 +1,214 @@
+// kernels_fft.cu -- G1 FFT stages on row-interleaved tiles, and the
+// reference <-> tile conversions.
+//
+// One warp per (butterfly, group of 32 rows): the twiddle of a butterfly is
+// the same for all 32 rows, so its GLV/NAF program (scalar_prog.cuh) runs
+// warp-uniformly.  The reference instead gives each thread a different
+// butterfly of one row (g1p_fft.cu:25-177), so a 256-bit double-and-add per
+// thread with divergent bits.  The two GLV base points of each thread live in
+// a conflict-free shared-memory slot (word k of thread t at [k][t]).
+#include "consts.cuh"
+#include "launch.h"
+#include "layout.cuh"
+
+namespace fk {
+
+cudaError_t upload_consts_fft() { return upload_module_consts(); }
+
+constexpr int FFT_THREADS = 128;
+
+// kind 0: DIF with inverse twiddles (natural in, bit-reversed out, no 1/m);
+// kind 1: DIT with forward twiddles (bit-reversed in, natural out).
+template <int KIND>
+__global__ void __launch_bounds__(FFT_THREADS) k_g1_stage(uint4 *__restrict__ D, int G, int log_m, int s) {
+    __shared__ uint32_t slots[72][FFT_THREADS];
+    const int m = 1 << log_m;
+    const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const int g = warp % G, b = warp / G;
+    if (b >= (m >> 1)) return;
+    int half, tix;
+    if (KIND == 0) {
+        half = m >> (s + 1);
+        const int j = b & (half - 1);
+        tix = ((m - (j << s)) << (MAX_LOG_M - log_m)) & 511;  // w_m^-(j 2^s) as a power of w_512
+    } else {
+        half = 1 << s;
+        const int j = b & (half - 1);
+        tix = (j << (log_m - 1 - s)) << (MAX_LOG_M - log_m);
+    }
+    const int j = b & (half - 1);
+    const int i0 = ((b / half) * 2 * half) + j, i1 = i0 + half;
+    uint4 *p0 = D + tile_index(g, m, i0);
+    uint4 *p1 = D + tile_index(g, m, i1);
+    const StridedPoint sP{&slots[0][threadIdx.x], FFT_THREADS}, sPhi{&slots[36][threadIdx.x], FFT_THREADS};
+    if (KIND == 0) {
+        // x = u + v, y = (u - v) * w^-t
+        G1P u, x;
+        tile_load(u, p0, lane);
+        {
+            G1P v;
+            tile_load(v, p1, lane);
+            sP.put(v);
+        }
+        g1_add_q(x, u, sP, false);
+        tile_store(p0, lane, x);
+        g1_add_q(x, u, sP, true);
+        if (tix != 0) {
+            sP.put(x);
+            g1_mul_prog(x, sP, sPhi, c_prog[tix]);
+        }
+        tile_store(p1, lane, x);
+    } else {
+        // v' = v * w^t, x = u + v', y = u - v'
+        G1P u, x;
+        {
+            G1P v;
+            tile_load(v, p1, lane);
+            if (tix != 0) {
+                sP.put(v);
+                g1_mul_prog(v, sP, sPhi, c_prog[tix]);
+            }
+            sP.put(v);
+        }
+        tile_load(u, p0, lane);
+        g1_add_q(x, u, sP, false);
+        tile_store(p0, lane, x);
+        g1_add_q(x, u, sP, true);
+        tile_store(p1, lane, x);
+    }
+}
+
+// last DIF stage + zeroing of the upper half + first DIT stage: pairs
+// (2q, 2q+1) -> both = a + b, optionally times 2^-log_m
+template <bool SCALE>
+__global__ void __launch_bounds__(FFT_THREADS) k_g1_middle(uint4 *__restrict__ D, int G, int log_m) {
+    __shared__ uint32_t slots[SCALE ? 72 : 1][FFT_THREADS];
+    const int m = 1 << log_m;
+    const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const int g = warp % G, q = warp / G;
+    if (q >= (m >> 1)) return;
+    uint4 *p0 = D + tile_index(g, m, 2 * q);
+    uint4 *p1 = D + tile_index(g, m, 2 * q + 1);
+    G1P u, v, x;
+    tile_load(u, p0, lane);
+    tile_load(v, p1, lane);
+    g1_add(x, u, v);
+    if (SCALE) {
+        const StridedPoint sP{&slots[0][threadIdx.x], FFT_THREADS}, sPhi{&slots[SCALE ? 36 : 0][threadIdx.x], FFT_THREADS};
+        sP.put(x);
+        g1_mul_prog(x, sP, sPhi, c_prog[512 + log_m]);
+    }
+    tile_store(p0, lane, x);
+    tile_store(p1, lane, x);
+}
+
+// every point of the tiles times program `prog`
+__global__ void __launch_bounds__(FFT_THREADS) k_g1_scale(uint4 *__restrict__ D, int G, int log_m, int prog) {
+    __shared__ uint32_t slots[72][FFT_THREADS];
+    const int m = 1 << log_m;
+    const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const int g = warp % G, i = warp / G;
+    if (i >= m) return;
+    uint4 *p = D + tile_index(g, m, i);
+    const StridedPoint sP{&slots[0][threadIdx.x], FFT_THREADS}, sPhi{&slots[36][threadIdx.x], FFT_THREADS};
+    G1P u;
+    tile_load(u, p, lane);
+    sP.put(u);
+    g1_mul_prog(u, sP, sPhi, c_prog[prog]);
+    tile_store(p, lane, u);
+}
+
+// reference g1p_t rows [rows][m] -> tiles.  bitrev_in: element i goes to
+// position bitrev(i); zero_upper: elements i >= m/2 taken as infinity.
+// Lanes of padding rows hold infinity.
+__global__ void k_ref_to_tile(uint4 *__restrict__ D, const uint64_t *__restrict__ src, int rows, int G, int log_m,
+                              int bitrev_in, int zero_upper) {
+    const int m = 1 << log_m;
+    const size_t total = (size_t)G * 32 * m;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int row = (int)(e / m), i = (int)(e % m);
+        G1P p;
+        if (row < rows && !(zero_upper && i >= (m >> 1))) g1p_from_ref(p, src + 18 * e);
+        else g1_set_inf(p);
+        const int pos = bitrev_in ? (int)bitrev((unsigned)i, log_m) : i;
+        tile_store(D + tile_index(row >> 5, m, pos), row & 31, p);
+    }
+}
+
+// tiles -> reference g1p_t rows, natural order; row r is written at
+// dst + 18 * (row_off ? row_off[r] : r * m)
+__global__ void k_tile_to_ref(uint64_t *__restrict__ dst, const uint4 *__restrict__ D, const size_t *__restrict__ row_off,
+                              int rows, int log_m, int bitrev_out) {
+    const int m = 1 << log_m;
+    const size_t total = (size_t)rows * m;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int row = (int)(e / m), i = (int)(e % m);
+        const int pos = bitrev_out ? (int)bitrev((unsigned)i, log_m) : i;
+        G1P p;
+        tile_load(p, D + tile_index(row >> 5, m, pos), row & 31);
+        const size_t base = row_off ? row_off[row] : (size_t)row * m;
+        g1p_to_ref(dst + 18 * (base + i), p);
+    }
+}
+
+// h[row][m/2 .. m-1] = infinity, in place (fk20_hext2h, fk20_poly2h_fft.cu:27-33)
+__global__ void k_hext2h_ref(uint64_t *__restrict__ h, int rows, int log_m) {
+    const int m = 1 << log_m;
+    const size_t total = (size_t)rows * (m >> 1);
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t row = e / (m >> 1), i = (m >> 1) + e % (m >> 1);
+        uint64_t *gp = h + 18 * (row * m + i);
+#pragma unroll
+        for (int k = 0; k < 18; k++) gp[k] = 0;
+        gp[6] = 1;
+    }
+}
+
+// setup -> bit-reversed FFT input tiles for xext_fft: lane i < 16, position j:
+// x_j = setup[n - l - 1 - i - l j] for j < k - 1, else infinity
+// (FK20Py/fk20_multi_cuda.py:104-109, fk20_single.py:45-58)
+__global__ void k_setup_to_tile(uint4 *D, const uint64_t *setup, int n, int log_m) {
+    const int m = 1 << log_m;
+    const int k = n / L_COLS;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 32 * m; e += gridDim.x * blockDim.x) {
+        const int lane = e / m, j = e % m;
+        G1P p;
+        if (lane < L_COLS && j < k - 1) g1p_from_ref(p, setup + 18 * (size_t)(n - L_COLS - 1 - lane - L_COLS * j));
+        else g1_set_inf(p);
+        tile_store(D + tile_index(0, m, (int)bitrev((unsigned)j, log_m)), lane, p);
+    }
+}
+
+void launch_g1_stage(uint4 *D, int G, int log_m, int s, int kind, cudaStream_t st) {
+    const unsigned blocks = blocks_for((size_t)G * ((1u << log_m) / 2), FFT_THREADS / 32);
+    if (kind == 0) k_g1_stage<0><<<blocks, FFT_THREADS, 0, st>>>(D, G, log_m, s);
+    else k_g1_stage<1><<<blocks, FFT_THREADS, 0, st>>>(D, G, log_m, s);
+}
+void launch_g1_middle(uint4 *D, int G, int log_m, int scale, cudaStream_t st) {
+    const unsigned blocks = blocks_for((size_t)G * ((1u << log_m) / 2), FFT_THREADS / 32);
+    if (scale) k_g1_middle<true><<<blocks, FFT_THREADS, 0, st>>>(D, G, log_m);
+    else k_g1_middle<false><<<blocks, FFT_THREADS, 0, st>>>(D, G, log_m);
+}
+void launch_g1_scale(uint4 *D, int G, int log_m, int prog, cudaStream_t st) {
+    k_g1_scale<<<blocks_for((size_t)G * (1u << log_m), FFT_THREADS / 32), FFT_THREADS, 0, st>>>(D, G, log_m, prog);
+}
+void launch_ref_to_tile(uint4 *D, const uint64_t *src, int rows, int G, int log_m, int bitrev_in, int zero_upper,
+                        cudaStream_t st) {
+    k_ref_to_tile<<<grid_stride_blocks((size_t)G * 32 * (1u << log_m)), 256, 0, st>>>(D, src, rows, G, log_m,
+                                                                                   bitrev_in, zero_upper);
+}
+void launch_tile_to_ref(uint64_t *dst, const uint4 *D, const size_t *row_off, int rows, int log_m, int bitrev_out,
+                        cudaStream_t st) {
+    k_tile_to_ref<<<grid_stride_blocks((size_t)rows << log_m), 256, 0, st>>>(dst, D, row_off, rows, log_m, bitrev_out);
+}
+void launch_hext2h_ref(uint64_t *h, int rows, int log_m, cudaStream_t st) {
+    k_hext2h_ref<<<grid_stride_blocks((size_t)rows << (log_m - 1)), 256, 0, st>>>(h, rows, log_m);
+}
+void launch_setup_to_tile(uint4 *D, const uint64_t *setup, int n, int log_m, cudaStream_t st) {
+    k_setup_to_tile<<<grid_stride_blocks((size_t)32 << log_m), 256, 0, st>>>(D, setup, n, log_m);
+}
+
+}  // namespace fk

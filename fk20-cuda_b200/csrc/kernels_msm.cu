@@ -1,0 +1,82 @@
+// kernels_msm.cu -- fixed-base MSM of the FK20 pipeline.
+//
+// hext_fft[row][c] = sum_{i<16} tc_fft[row][i][c] * X_i[c]  (fk20_msm.cu:23-66;
+// FK20Py/fk20_single.py:73-76).  The bases X_i[c] are fixed per setup, so each
+// has a table of its signed-digit multiples: entry (w, e) = (e+1) 2^(cb w) X,
+// e < 2^(cb-1), affine Montgomery (built by kernels_tables.cu).  A 255-bit
+// scalar is recoded on the fly into ceil(255/cb) signed digits in
+// [-2^(cb-1), 2^(cb-1)] and each nonzero digit costs one mixed addition
+// (RCB Algorithm 8) of a gathered 96-byte entry: no doublings at all, against
+// ~255 doublings + ~128 additions per term in the reference's g1p_mul loop.
+// One warp per (column c, group of 32 rows); lanes are rows.
+#include "consts.cuh"
+#include "launch.h"
+#include "layout.cuh"
+
+namespace fk {
+
+cudaError_t upload_consts_msm() { return upload_module_consts(); }
+
+__global__ void __launch_bounds__(128) k_msm(MsmArgs a) {
+    const int m = 1 << a.log_m;
+    const int warp = blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const int g = warp % a.G, c = warp / a.G;
+    if (c >= m) return;
+    const int row = g * 32 + lane;
+    const bool live = row < a.rows;
+    const int E = 1 << (a.cb - 1);
+    const uint32_t mask = (1u << a.cb) - 1u;
+    G1P acc;
+    g1_set_inf(acc);
+    for (int i = 0; i < L_COLS; i++) {
+        uint32_t s[9];
+        const uint4 *src = a.S + ((((size_t)g * m + c) * L_COLS + i) * SCAL_Q) * 32 + lane;
+        const uint4 v0 = src[0], v1 = src[32];
+        s[0] = v0.x; s[1] = v0.y; s[2] = v0.z; s[3] = v0.w;
+        s[4] = v1.x; s[5] = v1.y; s[6] = v1.z; s[7] = v1.w;
+        s[8] = 0;
+        if (!live) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) s[k] = 0;
+        }
+        const uint4 *tb = a.table + ((size_t)(i * m + c) * a.W) * E * 6;
+        int carry = 0;
+        for (int w = 0; w < a.W; w++) {
+            const int bit = w * a.cb;
+            const int wd = bit >> 5, sh = bit & 31;
+            uint32_t raw = s[wd] >> sh;
+            if (sh + a.cb > 32) raw |= s[wd + 1] << (32 - sh);
+            int d = (int)(raw & mask) + carry;
+            carry = d > E;
+            if (carry) d -= (1 << a.cb);
+            if (d != 0) {
+                const int e = (d < 0 ? -d : d) - 1;
+                const uint4 *ent = tb + ((size_t)w * E + e) * 6;
+                Fp x, y;
+                const uint4 q0 = ent[0], q1 = ent[1], q2 = ent[2], q3 = ent[3], q4 = ent[4], q5 = ent[5];
+                x.w[0] = q0.x; x.w[1] = q0.y; x.w[2] = q0.z; x.w[3] = q0.w;
+                x.w[4] = q1.x; x.w[5] = q1.y; x.w[6] = q1.z; x.w[7] = q1.w;
+                x.w[8] = q2.x; x.w[9] = q2.y; x.w[10] = q2.z; x.w[11] = q2.w;
+                y.w[0] = q3.x; y.w[1] = q3.y; y.w[2] = q3.z; y.w[3] = q3.w;
+                y.w[4] = q4.x; y.w[5] = q4.y; y.w[6] = q4.z; y.w[7] = q4.w;
+                y.w[8] = q5.x; y.w[9] = q5.y; y.w[10] = q5.z; y.w[11] = q5.w;
+                // an entry (0, 0) encodes a base at infinity (not on the curve)
+                if (!(f_is_zero(x) && f_is_zero(y))) {
+                    if (d < 0) f_neg(y, y);
+                    g1_madd(acc, acc, x, y);
+                }
+            }
+        }
+    }
+    if (a.times_m) {
+        for (int k = 0; k < a.log_m; k++) g1_dbl(acc, acc);
+    }
+    tile_store(a.D + tile_index(g, m, c), lane, acc);
+}
+
+void launch_msm(const MsmArgs &a, cudaStream_t st) {
+    k_msm<<<blocks_for((size_t)a.G * (1u << a.log_m), 4), 128, 0, st>>>(a);
+}
+
+}  // namespace fk

@@ -1,0 +1,191 @@
+/*
+ * fk20_b200.h -- C ABI of the B200 FK20 engine (libfk20b200.so).
+ *
+ * Drop-in for the FK20 hot path of lCardosoSantos/FK20-CUDA: every amortized
+ * KZG proof of a batch of polynomials against one shared setup.  Entry-point
+ * names and argument meanings follow the reference (fk20.cuh:20-38,
+ * fr.cuh:62-69, g1.cuh:98-108); the reference's __global__ kernels, which a
+ * caller launched with <<<rows, 256, smem>>>, become host launchers here.
+ *
+ * Conventions (all entry points):
+ *  - Buffers are DEVICE pointers in the reference layouts: fr_t = 4 x uint64,
+ *    fp_t = 6 x uint64, g1p_t = {x, y, z} homogeneous projective (x = X/Z,
+ *    y = Y/Z), little-endian, standard (non-Montgomery) form.  Inputs may be
+ *    any representative (fp_t < 2^384, fr_t < 2^256, like the reference);
+ *    outputs are canonical (< p, < r), and a point at infinity is written as
+ *    (0, 1, 0) (g1p.cu:95-100).  G1 inputs must lie in the order-r subgroup
+ *    (true of every FK20 value: setup multiples and their combinations).
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream);
+ *    work is enqueued asynchronously, like the reference's launches.
+ *  - Return value: 0 on success, a cudaError_t value (1..999) for a CUDA
+ *    failure, or one of the FK20_E* codes below for a rejected argument.
+ *    Nothing traps; arguments are validated on the host before any launch.
+ *  - The l = 16 chunking of the reference is fixed; polynomial length
+ *    n in {1024, 2048, 4096} gives FFT size m = 2n/16 in {128, 256, 512}.
+ *    The reference entry points without an `n` argument use n = 4096, m = 512.
+ */
+#ifndef FK20_B200_H
+#define FK20_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef uint64_t fr_t[4];
+typedef uint64_t fp_t[6];
+typedef struct { fp_t x, y; } g1a_t;
+typedef struct { fp_t x, y, z; } g1p_t;
+
+#define FK20_OK 0
+#define FK20_EINVAL 1001   /* bad size, row count, null pointer or alignment */
+#define FK20_ENOSETUP 1002 /* context has no tables for this polynomial length */
+#define FK20_ENOMEM 1003   /* device allocation failed */
+#define FK20_ENODEV 1004   /* no usable sm_100 device */
+
+/* ------------------------------------------------------------------ context
+ * A context owns, on one device, the fixed-base tables built from xext_fft
+ * (one set per polynomial length) and the per-call workspaces.  Calls on one
+ * context are serialised by an internal lock and run in stream order; use one
+ * context per concurrent stream.  No reference counterpart: the reference keeps
+ * this state in file-scope __managed__ arrays (fk20_poly2h_fft.cu:15-16,
+ * fk20_msm.cu:357-360), which is why it is not re-entrant.
+ */
+typedef struct fk20_ctx fk20_ctx;
+
+/* window: signed-digit width of the fixed-base tables (8..13; 0 = default 10).
+ * Table bytes per polynomial length n: 16*m bases * ceil(255/w) windows *
+ * 2^(w-1) entries * 96 B (10.5 GB for n = 4096, w = 10). */
+int fk20_ctx_create(fk20_ctx **ctx, int device, int window);
+int fk20_ctx_destroy(fk20_ctx *ctx);
+
+/* Build the tables of length n from xext_fft[16][m] (device, g1p_t).
+ * Replaces fk20_msm_makelut (fk20_msm.cu:79-141). */
+int fk20_ctx_load_xext_fft(fk20_ctx *ctx, unsigned n, const g1p_t *xext_fft, void *stream);
+
+/* xext_fft[16][m] from the setup s_0..s_{n-1} (device g1p_t) on the GPU, then
+ * build the tables.  Replaces the reference's fk20_setup2xext_fft (fk20.cu:28-59,
+ * which its own comment marks as failing) and the Python precompute
+ * FK20Py/fk20_multi_cuda.py:104-109. */
+int fk20_ctx_load_setup(fk20_ctx *ctx, unsigned n, const g1p_t *setup, void *stream);
+
+/* h_fft[rows][m] (the m = 2n/16 proofs of each row) for rows x n polynomial
+ * coefficients, against the context's tables for n.  Same computation as the
+ * reference's host pipeline fk20_poly2h_fft (fk20_poly2h_fft.cu:47-78). */
+int fk20_ctx_poly2h_fft(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polynomial, unsigned rows, unsigned n,
+                        void *stream);
+
+/* Same, with intermediate hext_fft[rows][m] also written (may be NULL). */
+int fk20_ctx_poly2hext_fft(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *polynomial, unsigned rows, unsigned n,
+                           void *stream);
+
+/* MSM stage alone: hext_fft[rows][m] = sum_i tc_fft[row][i][c] * xext_fft[i][c]
+ * for tc_fft[rows][16][m] (fk20_msm.cu:23-66). */
+int fk20_ctx_msm(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *tc_fft, unsigned rows, unsigned n, void *stream);
+
+/* Ragged batch: `count` independent FK20 instances, instance j with length
+ * n_j in {1024, 2048, 4096}, polynomial at poly_off[j] (in fr_t units from
+ * `polys`) and m_j proofs written at out_off[j] (in g1p_t units from `h_fft`).
+ * All offset arrays are HOST arrays.  Instances are grouped by length and run
+ * as one stream-ordered batch per length. */
+int fk20_ctx_batch(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polys, unsigned count, const unsigned *n,
+                   const size_t *poly_off, const size_t *out_off, void *stream);
+
+/* Device bytes the context holds (tables + workspaces). */
+size_t fk20_ctx_device_bytes(const fk20_ctx *ctx);
+
+/* ------------------------------------------------------------------ reference entry points
+ * These use a process-wide default context on the current device; tables are
+ * rebuilt when the content of xext_fft changes (checked by a device-side
+ * fingerprint).  n = 4096, m = 512, rows <= 2^20.
+ */
+
+/* fk20_poly2h_fft.cu:47 -- polynomial[rows][4096] + xext_fft[16][512] -> h_fft[rows][512] */
+int fk20_poly2h_fft(g1p_t *h_fft, const fr_t *polynomial, const g1p_t *xext_fft, unsigned rows);
+
+/* fk20_poly2toeplitz_coefficients.cu:25 -- polynomial[rows][4096] -> tc[rows][16][512] */
+int fk20_poly2toeplitz_coefficients(fr_t *toeplitz_coefficients, const fr_t *polynomial, unsigned rows,
+                                    void *stream);
+
+/* fk20_poly2toeplitz_coefficients_fft.cu:24 -- polynomial -> tc_fft[rows][16][512] */
+int fk20_poly2toeplitz_coefficients_fft(fr_t *toeplitz_coefficients_fft, const fr_t *polynomial, unsigned rows,
+                                        void *stream);
+
+/* fk20_poly2hext_fft.cu:26 -- polynomial + xext_fft -> hext_fft[rows][512] */
+int fk20_poly2hext_fft(g1p_t *hext_fft, const fr_t *polynomial, const g1p_t *xext_fft, unsigned rows, void *stream);
+
+/* fk20_msm.cu:23 -- tc_fft[rows][16][512] + xext_fft[16][512] -> hext_fft[rows][512] */
+int fk20_msm(g1p_t *hext_fft, const fr_t *toeplitz_coefficients_fft, const g1p_t *xext_fft, unsigned rows,
+             void *stream);
+
+/* fk20_hext_fft2h_fft.cu:27 -- hext_fft[rows][512] -> h_fft[rows][512]
+ * (inverse FFT, upper half set to infinity, forward FFT) */
+int fk20_hext_fft2h_fft(g1p_t *h_fft, const g1p_t *hext_fft, unsigned rows, void *stream);
+
+/* fk20.cuh:24 -- hext_fft -> h (inverse FFT, upper half infinity) */
+int fk20_hext_fft2h(g1p_t *h, const g1p_t *hext_fft, unsigned rows, void *stream);
+
+/* fk20.cu:74 -- hext_fft -> hext (inverse FFT) */
+int fk20_hext_fft2hext(g1p_t *hext, const g1p_t *hext_fft, unsigned rows, void *stream);
+
+/* fk20.cu:94 -- h -> h_fft (forward FFT) */
+int fk20_h2h_fft(g1p_t *h_fft, const g1p_t *h, unsigned rows, void *stream);
+
+/* fk20_poly2h_fft.cu:27 -- h[rows][512]: entries 256..511 set to infinity, in place */
+int fk20_hext2h(g1p_t *h, unsigned rows, void *stream);
+
+/* fk20.cu:28 -- setup[>= 4080] -> xext_fft[16][512] */
+int fk20_setup2xext_fft(g1p_t *xext_fft, const g1p_t *setup, void *stream);
+
+/* fr_fft.cu:318 / :347 (fr_fft_wrapper, fr_ift_wrapper) -- `count` independent
+ * 512-point transforms over Fr, natural order in and out; the inverse includes
+ * the 1/512 factor.  Input and output may alias. */
+int fr_fft(fr_t *output, const fr_t *input, unsigned count, void *stream);
+int fr_ift(fr_t *output, const fr_t *input, unsigned count, void *stream);
+
+/* g1p_fft.cu:337 / :350 (g1p_fft_wrapper, g1p_ift_wrapper) -- `count`
+ * independent 512-point transforms over G1, natural order; the inverse
+ * includes the 1/512 factor.  Input and output may alias. */
+int g1p_fft(g1p_t *output, const g1p_t *input, unsigned count, void *stream);
+int g1p_ift(g1p_t *output, const g1p_t *input, unsigned count, void *stream);
+
+/* Size-generic transforms: log_m in 1..9. */
+int fr_fft_n(fr_t *output, const fr_t *input, unsigned log_m, unsigned count, int inverse, void *stream);
+int g1p_fft_n(g1p_t *output, const g1p_t *input, unsigned log_m, unsigned count, int inverse, void *stream);
+
+/* ------------------------------------------------------------------ element-wise helpers
+ * Batched forms of the fp_* / fr_* / g1p_* device API (fp.cuh:16-41,
+ * fr.cuh:33-58, g1.cuh:31-96), for tests, microbenchmarks and callers that
+ * need single operations.  op codes:
+ *   field: 0 mul, 1 sqr, 2 add, 3 sub, 4 neg, 5 inv, 6 reduce (canonical),
+ *          7 x2, 8 x3, 9 x4, 10 x8, 11 x12
+ *   g1p:   0 add, 1 dbl, 2 neg, 3 sub, 4 mul by fr_t scalar, 5 normalise
+ *          (affine {x, y, 1}, infinity (0, 1, 0)), 6 is_point (b: uint8 out)
+ */
+int fp_op_n(int op, fp_t *out, const fp_t *a, const fp_t *b, size_t count, void *stream);
+int fr_op_n(int op, fr_t *out, const fr_t *a, const fr_t *b, size_t count, void *stream);
+int g1p_op_n(int op, g1p_t *out, const g1p_t *a, const void *b, size_t count, void *stream);
+
+/* fr.cu:99 / g1p.cu:142 -- eq[i] = (x[i] == y[i]) mathematically */
+int fr_eq_n(uint8_t *eq, const fr_t *x, const fr_t *y, size_t count, void *stream);
+int g1p_eq_n(uint8_t *eq, const g1p_t *p, const g1p_t *q, size_t count, void *stream);
+
+/* g1p.cu:168 -- affine conversion of count points (infinity -> (0, 0)) */
+int g1a_fromG1p_n(g1a_t *a, const g1p_t *p, size_t count, void *stream);
+
+/* Microbenchmark of the Montgomery product: `iters` dependent products per
+ * element on `count` elements of limb-major Montgomery data (field 0 = Fp,
+ * 1 = Fr; sqr != 0 squares).  data: count x N 32-bit words, limb-major
+ * (word k of element e at data[k * count + e]). */
+int fk20_bench_field(int field, int sqr, uint32_t *data, size_t count, int iters, void *stream);
+
+/* Engine version string. */
+const char *fk20_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FK20_B200_H */

@@ -1,0 +1,97 @@
+// Host build of the engine's field and curve code (csrc/field.cuh, g1.cuh)
+// with the carry flag emulated in C -- CPU unit tests only.  Lets the limb
+// schedules, reduction bounds and curve formulas be checked against the
+// oracle without a GPU.  Standard-form uint64 I/O, reference layouts.
+#include <cstring>
+#include "field.cuh"
+#include "g1.cuh"
+
+using namespace fk;
+
+template <class F>
+static void load(Elem<F> &e, const uint64_t *x) {
+    for (int i = 0; i < F::N / 2; i++) { e.w[2 * i] = (uint32_t)x[i]; e.w[2 * i + 1] = (uint32_t)(x[i] >> 32); }
+}
+template <class F>
+static void store(uint64_t *x, const Elem<F> &e) {
+    for (int i = 0; i < F::N / 2; i++) x[i] = (uint64_t)e.w[2 * i] | ((uint64_t)e.w[2 * i + 1] << 32);
+}
+
+template <class F>
+static int field_op(int op, uint64_t *out, const uint64_t *a, const uint64_t *b, long count) {
+    const int L = F::N / 2;
+    for (long i = 0; i < count; i++) {
+        Elem<F> x, y, z, t;
+        load(t, a + L * i);
+        f_to_mont(x, t);
+        if (b) { load(t, b + L * i); f_to_mont(y, t); } else { f_set_zero(y); }
+        switch (op) {
+        case 0: f_mul(z, x, y); break;
+        case 1: f_sqr(z, x); break;
+        case 2: f_add(z, x, y); break;
+        case 3: f_sub(z, x, y); break;
+        case 4: f_neg(z, x); break;
+        case 5: f_inv(z, x); break;
+        case 6: z = x; break;
+        case 7: f_dbl(z, x); break;
+        case 11: f_mul12(z, x); break;
+        default: return -1;
+        }
+        f_from_mont(t, z);
+        store(out + L * i, t);
+    }
+    return 0;
+}
+
+static void g1_load(G1P &p, const uint64_t *g) {
+    Fp t;
+    load(t, g); f_to_mont(p.x, t);
+    load(t, g + 6); f_to_mont(p.y, t);
+    load(t, g + 12); f_to_mont(p.z, t);
+}
+static void g1_store(uint64_t *g, const G1P &p) {
+    Fp t;
+    f_from_mont(t, p.x); store(g, t);
+    f_from_mont(t, p.y); store(g + 6, t);
+    f_from_mont(t, p.z); store(g + 12, t);
+}
+
+extern "C" {
+int emul_fp_op(int op, uint64_t *out, const uint64_t *a, const uint64_t *b, long count) { return field_op<FpDesc>(op, out, a, b, count); }
+int emul_fr_op(int op, uint64_t *out, const uint64_t *a, const uint64_t *b, long count) { return field_op<FrDesc>(op, out, a, b, count); }
+
+// op: 0 add, 1 dbl, 2 madd (b affine: x,y of 12 limbs), 3 phi, 4 neg
+int emul_g1_op(int op, uint64_t *out, const uint64_t *a, const uint64_t *b, long count) {
+    for (long i = 0; i < count; i++) {
+        G1P p, q, r;
+        g1_load(p, a + 18 * i);
+        switch (op) {
+        case 0: g1_load(q, b + 18 * i); g1_add(r, p, q); break;
+        case 1: g1_dbl(r, p); break;
+        case 2: { Fp qx, qy, t; load(t, b + 12 * i); f_to_mont(qx, t); load(t, b + 12 * i + 6); f_to_mont(qy, t); g1_madd(r, p, qx, qy); } break;
+        case 3: g1_phi(r, p); break;
+        case 4: g1_neg(r, p); break;
+        default: return -1;
+        }
+        g1_store(out + 18 * i, r);
+    }
+    return 0;
+}
+}
+
+#include "scalar_prog.cuh"
+extern "C" {
+// [k] P through a GLV/NAF program built for k (standard form, 4 x u64)
+int emul_g1_mul_prog(uint64_t *out, const uint64_t *pts, const uint64_t *k, long count, int *dbl, int *add) {
+    uint32_t prog[PROG_WORDS];
+    host::make_program(prog, k);
+    host::program_cost(prog, dbl, add);
+    for (long i = 0; i < count; i++) {
+        G1P p, r;
+        g1_load(p, pts + 18 * i);
+        g1_mul_prog(r, p, prog);
+        g1_store(out + 18 * i, r);
+    }
+    return 0;
+}
+}
