@@ -179,12 +179,71 @@ struct Tables {
 
 }  // namespace
 
+// Per-launch profiling: CUDA events on the launching stream around every
+// pipeline kernel, with the algorithmic work of that launch (in 32x32->64-bit
+// limb products: Fp product M_p = 300, Fr product M_r = 136, RCB addition
+// 12 M_p, mixed addition 11 M_p, doubling 8 M_p).
+struct Profiler {
+    bool on = false;
+    struct Rec {
+        int kind;
+        double products;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    double ms[FK20_NKINDS] = {0}, products[FK20_NKINDS] = {0};
+    long launches[FK20_NKINDS] = {0};
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int kind, double prod, cudaStream_t st) {
+        if (!on) return;
+        Rec r{kind, prod, get(), get()};
+        cudaEventRecord(r.a, st);
+        pending.push_back(r);
+    }
+    void end(cudaStream_t st) {
+        if (!on || pending.empty()) return;
+        cudaEventRecord(pending.back().b, st);
+    }
+    void collect() {
+        for (Rec &r : pending) {
+            cudaEventSynchronize(r.b);
+            float t = 0;
+            cudaEventElapsedTime(&t, r.a, r.b);
+            ms[r.kind] += t;
+            products[r.kind] += r.products;
+            launches[r.kind] += 1;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        pending.clear();
+    }
+    void reset() {
+        collect();
+        for (int k = 0; k < FK20_NKINDS; k++) ms[k] = products[k] = 0, launches[k] = 0;
+    }
+    ~Profiler() {
+        for (Rec &r : pending) pool.push_back(r.a), pool.push_back(r.b);
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    }
+};
+
 struct fk20_ctx {
     int device = 0;
     int window = 10;
     std::mutex mu;
     Tables tab[3];  // log_m 7, 8, 9
     DevBuf S, D, D2, scratch, xext, offs, fp_dev;
+    Profiler prof;
 };
 
 namespace {
@@ -205,19 +264,67 @@ struct DeviceGuard {  // make ctx->device current for the duration of a call
     }
 };
 
+// ---- algorithmic work model (limb products) ----------------------------------
+constexpr double MP = 300.0, MR = 136.0, ADD_P = 12 * MP, MADD_P = 11 * MP, DBL_P = 8 * MP;
+
+double prog_products(int idx) {
+    const HostConsts &hc = host_consts();
+    if (hc.prog[idx][0] & 0x300u) return 0.0;
+    return hc.prog_dbl[idx] * DBL_P + hc.prog_add[idx] * ADD_P + MP;  // + phi(P)
+}
+
+// one stage over `rows` rows: kind 0 DIF inverse, 1 DIT forward
+double stage_products(int rows, int log_m, int s, int kind) {
+    const int m = 1 << log_m;
+    double per_row = 0;
+    for (int b = 0; b < m / 2; b++) {
+        int tix;
+        if (kind == 0) {
+            const int half = m >> (s + 1), j = b & (half - 1);
+            tix = ((m - (j << s)) << (MAX_LOG_M - log_m)) & 511;
+        } else {
+            const int half = 1 << s, j = b & (half - 1);
+            tix = (j << (log_m - 1 - s)) << (MAX_LOG_M - log_m);
+        }
+        per_row += 2 * ADD_P + (tix ? prog_products(tix) : 0.0);
+    }
+    return per_row * rows;
+}
+
+double fr_fft_products(int log_m) {  // nontrivial twiddle products of one Fr FFT-m
+    const int m = 1 << log_m;
+    return ((double)log_m * (m / 2) - (m - 1)) * MR;
+}
+
 // inverse DIF stages 0..L-2, middle (last inverse + zero upper half + first
 // forward stage, optionally times 1/m), forward DIT stages 1..L-1
-int run_hext_to_hfft(uint4 *D, int G, int log_m, int scale, cudaStream_t st) {
+int run_hext_to_hfft(Profiler &pf, uint4 *D, int G, int rows, int log_m, int scale, cudaStream_t st) {
+    const int m = 1 << log_m;
     for (int s = 0; s < log_m - 1; s++) {
+        pf.begin(FK20_K_STAGE_INV, stage_products(rows, log_m, s, 0), st);
         launch_g1_stage(D, G, log_m, s, 0, st);
+        pf.end(st);
         CKL();
     }
+    pf.begin(FK20_K_MIDDLE, (double)rows * (m / 2) * (ADD_P + (scale ? prog_products(512 + log_m) : 0.0)), st);
     launch_g1_middle(D, G, log_m, scale, st);
+    pf.end(st);
     CKL();
     for (int s = 1; s < log_m; s++) {
+        pf.begin(FK20_K_STAGE_FWD, stage_products(rows, log_m, s, 1), st);
         launch_g1_stage(D, G, log_m, s, 1, st);
+        pf.end(st);
         CKL();
     }
+    return 0;
+}
+
+int output_launch(Profiler &pf, uint64_t *dst, const uint4 *D, const size_t *row_off, int rows, int log_m,
+                  int bitrev_out, cudaStream_t st) {
+    pf.begin(FK20_K_OUTPUT, (double)rows * (1 << log_m) * 3 * MP, st);
+    launch_tile_to_ref(dst, D, row_off, rows, log_m, bitrev_out, st);
+    pf.end(st);
+    CKL();
     return 0;
 }
 
@@ -266,7 +373,7 @@ int fingerprint(fk20_ctx *ctx, const void *p, size_t words, unsigned long long *
     return 0;
 }
 
-int msm_launch(Tables *T, uint4 *D, const uint4 *S, int G, int rows, int times_m, cudaStream_t st) {
+int msm_launch(Profiler &pf, Tables *T, uint4 *D, const uint4 *S, int G, int rows, int times_m, cudaStream_t st) {
     MsmArgs a;
     a.D = D;
     a.S = S;
@@ -277,7 +384,11 @@ int msm_launch(Tables *T, uint4 *D, const uint4 *S, int G, int rows, int times_m
     a.cb = T->cb;
     a.W = T->W;
     a.times_m = times_m;
+    const double prod = (double)rows * L_COLS * (1 << T->log_m) * T->W * MADD_P +
+                        (times_m ? (double)rows * (1 << T->log_m) * T->log_m * DBL_P : 0.0);
+    pf.begin(FK20_K_MSM, prod, st);
     launch_msm(a, st);
+    pf.end(st);
     CKL();
     return 0;
 }
@@ -289,9 +400,11 @@ int pipeline_to_hext(fk20_ctx *ctx, Tables *T, const fr_t *poly, const size_t *r
     const int G = (int)((rows + 31) / 32);
     CKR(ctx->S.reserve(scal_bytes(G, m)));
     CKR(ctx->D.reserve(tile_bytes(G, m)));
+    ctx->prof.begin(FK20_K_TC_FFT, (double)rows * L_COLS * fr_fft_products(log_m), st);
     launch_tc_fft((uint4 *)ctx->S.p, (const uint64_t *)poly, row_off, (int)T->n, log_m, rows, st);
+    ctx->prof.end(st);
     CKL();
-    CKR(msm_launch(T, (uint4 *)ctx->D.p, (const uint4 *)ctx->S.p, G, (int)rows, times_m, st));
+    CKR(msm_launch(ctx->prof, T, (uint4 *)ctx->D.p, (const uint4 *)ctx->S.p, G, (int)rows, times_m, st));
     return 0;
 }
 
@@ -416,6 +529,34 @@ int fk20_ctx_destroy(fk20_ctx *ctx) {
     return 0;
 }
 
+int fk20_ctx_profile(fk20_ctx *ctx, int enable) {
+    if (!ctx) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    ctx->prof.reset();
+    ctx->prof.on = enable != 0;
+    return 0;
+}
+
+int fk20_ctx_profile_read(fk20_ctx *ctx, int kind, double *ms, long *launches, double *products) {
+    if (!ctx || kind < 0 || kind >= FK20_NKINDS) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    ctx->prof.collect();
+    if (ms) *ms = ctx->prof.ms[kind];
+    if (launches) *launches = ctx->prof.launches[kind];
+    if (products) *products = ctx->prof.products[kind];
+    return 0;
+}
+
+int fk20_program_cost(int index, int *dbl, int *add) {
+    if (index < 0 || index >= NPROG || !dbl || !add) return FK20_EINVAL;
+    const HostConsts &hc = host_consts();
+    *dbl = hc.prog_dbl[index];
+    *add = hc.prog_add[index];
+    return 0;
+}
+
 size_t fk20_ctx_device_bytes(const fk20_ctx *ctx) {
     if (!ctx) return 0;
     size_t b = ctx->S.bytes + ctx->D.bytes + ctx->D2.bytes + ctx->scratch.bytes + ctx->xext.bytes + ctx->offs.bytes;
@@ -459,9 +600,8 @@ int fk20_ctx_poly2h_fft(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polynomial, uns
     cudaStream_t st = S_(stream);
     const int G = (int)((rows + 31) / 32);
     CKR(pipeline_to_hext(ctx, T, polynomial, nullptr, rows, 0, st));
-    CKR(run_hext_to_hfft((uint4 *)ctx->D.p, G, log_m, 0, st));
-    launch_tile_to_ref((uint64_t *)h_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st);
-    CKL();
+    CKR(run_hext_to_hfft(ctx->prof, (uint4 *)ctx->D.p, G, (int)rows, log_m, 0, st));
+    CKR(output_launch(ctx->prof, (uint64_t *)h_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st));
     return 0;
 }
 
@@ -477,8 +617,7 @@ int fk20_ctx_poly2hext_fft(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *polynomia
     if (!T->ready) return FK20_ENOSETUP;
     cudaStream_t st = S_(stream);
     CKR(pipeline_to_hext(ctx, T, polynomial, nullptr, rows, 1, st));
-    launch_tile_to_ref((uint64_t *)hext_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st);
-    CKL();
+    CKR(output_launch(ctx->prof, (uint64_t *)hext_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st));
     return 0;
 }
 
@@ -498,9 +637,8 @@ int fk20_ctx_msm(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *tc_fft, unsigned ro
     CKR(ctx->D.reserve(tile_bytes(G, m)));
     launch_ref_to_scalars((uint4 *)ctx->S.p, (const uint64_t *)tc_fft, (int)rows, log_m, st);
     CKL();
-    CKR(msm_launch(T, (uint4 *)ctx->D.p, (const uint4 *)ctx->S.p, G, (int)rows, 1, st));
-    launch_tile_to_ref((uint64_t *)hext_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st);
-    CKL();
+    CKR(msm_launch(ctx->prof, T, (uint4 *)ctx->D.p, (const uint4 *)ctx->S.p, G, (int)rows, 1, st));
+    CKR(output_launch(ctx->prof, (uint64_t *)hext_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st));
     return 0;
 }
 
@@ -536,10 +674,9 @@ int fk20_ctx_batch(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polys, unsigned coun
         Tables *T = tables_for(ctx, gr.log_m);
         const int G = (int)((gr.rows + 31) / 32);
         CKR(pipeline_to_hext(ctx, T, polys, doffs + gr.first, gr.rows, 0, st));
-        CKR(run_hext_to_hfft((uint4 *)ctx->D.p, G, gr.log_m, 0, st));
-        launch_tile_to_ref((uint64_t *)h_fft, (const uint4 *)ctx->D.p, doffs + gr.first + gr.rows, (int)gr.rows,
-                           gr.log_m, 0, st);
-        CKL();
+        CKR(run_hext_to_hfft(ctx->prof, (uint4 *)ctx->D.p, G, (int)gr.rows, gr.log_m, 0, st));
+        CKR(output_launch(ctx->prof, (uint64_t *)h_fft, (const uint4 *)ctx->D.p, doffs + gr.first + gr.rows,
+                          (int)gr.rows, gr.log_m, 0, st));
     }
     // the host offset array must outlive the copy from pageable memory
     CK(cudaStreamSynchronize(st));
@@ -640,7 +777,7 @@ int fk20_hext_fft2h_fft(g1p_t *h_fft, const g1p_t *hext_fft, unsigned rows, void
     uint4 *D = (uint4 *)ctx->D2.p;
     launch_ref_to_tile(D, (const uint64_t *)hext_fft, (int)rows, G, log_m, 0, 0, st);
     CKL();
-    CKR(run_hext_to_hfft(D, G, log_m, 1, st));
+    CKR(run_hext_to_hfft(ctx->prof, D, G, (int)rows, log_m, 1, st));
     launch_tile_to_ref((uint64_t *)h_fft, D, nullptr, (int)rows, log_m, 0, st);
     CKL();
     return 0;
@@ -715,6 +852,14 @@ int g1a_fromG1p_n(g1a_t *a, const g1p_t *p, size_t count, void *stream) {
     if (!a || !p || count == 0) return FK20_EINVAL;
     CKR(current_device_ready());
     launch_g1a_from_g1p((uint64_t *)a, (const uint64_t *)p, count, S_(stream));
+    CKL();
+    return 0;
+}
+
+int fk20_bench_imad(uint32_t *sink, int blocks, int threads, int iters, void *stream) {
+    if (!sink || blocks <= 0 || threads <= 0 || threads > 1024 || iters < 0) return FK20_EINVAL;
+    CKR(current_device_ready());
+    launch_bench_imad(sink, blocks, threads, iters, S_(stream));
     CKL();
     return 0;
 }

@@ -16,11 +16,16 @@ namespace fk {
 cudaError_t upload_consts_fft() { return upload_module_consts(); }
 
 constexpr int FFT_THREADS = 128;
+// minimum resident blocks per SM requested from ptxas for the stage kernels
+// (caps registers at 65536 / (FFT_THREADS * FK_FFT_MINB))
+#ifndef FK_FFT_MINB
+#define FK_FFT_MINB 1
+#endif
 
 // kind 0: DIF with inverse twiddles (natural in, bit-reversed out, no 1/m);
 // kind 1: DIT with forward twiddles (bit-reversed in, natural out).
 template <int KIND>
-__global__ void __launch_bounds__(FFT_THREADS) k_g1_stage(uint4 *__restrict__ D, int G, int log_m, int s) {
+__global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__restrict__ D, int G, int log_m, int s) {
     __shared__ uint32_t slots[72][FFT_THREADS];
     const int m = 1 << log_m;
     const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);

@@ -13,11 +13,15 @@
 #include "launch.h"
 #include "layout.cuh"
 
+#ifndef FK_MSM_MINB
+#define FK_MSM_MINB 1
+#endif
+
 namespace fk {
 
 cudaError_t upload_consts_msm() { return upload_module_consts(); }
 
-__global__ void __launch_bounds__(128) k_msm(MsmArgs a) {
+__global__ void __launch_bounds__(128, FK_MSM_MINB) k_msm(MsmArgs a) {
     const int m = 1 << a.log_m;
     const int warp = blockIdx.x * 4 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;

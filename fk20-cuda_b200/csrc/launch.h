@@ -58,6 +58,7 @@ void launch_fr_eq(uint8_t *eq, const uint64_t *x, const uint64_t *y, size_t coun
 void launch_g1p_eq(uint8_t *eq, const uint64_t *p, const uint64_t *q, size_t count, cudaStream_t st);
 void launch_g1a_from_g1p(uint64_t *a, const uint64_t *p, size_t count, cudaStream_t st);
 void launch_bench_field(int field, int sqr, uint32_t *data, size_t count, int iters, cudaStream_t st);
+void launch_bench_imad(uint32_t *sink, int blocks, int threads, int iters, cudaStream_t st);
 void launch_fingerprint(unsigned long long *out, const uint64_t *w, size_t n, cudaStream_t st);
 
 inline unsigned blocks_for(size_t work, unsigned per) {

@@ -35,7 +35,11 @@ ABI_SYMBOLS = (
     "fk20_hext_fft2h", "fk20_hext_fft2hext", "fk20_h2h_fft", "fk20_hext2h", "fk20_setup2xext_fft",
     "fr_fft", "fr_ift", "g1p_fft", "g1p_ift", "fr_fft_n", "g1p_fft_n", "fp_op_n", "fr_op_n",
     "g1p_op_n", "fr_eq_n", "g1p_eq_n", "g1a_fromG1p_n", "fk20_bench_field", "fk20_version",
+    "fk20_ctx_profile", "fk20_ctx_profile_read", "fk20_program_cost", "fk20_bench_imad",
 )
+
+# kernel kinds of the per-launch profiler (FK20_K_* in the header)
+KINDS = ("tc_fft", "msm", "stage_inv", "stage_fwd", "middle", "output")
 
 
 class Fk20Error(RuntimeError):
@@ -94,6 +98,11 @@ def lib() -> ctypes.CDLL:
             "g1a_fromG1p_n": ([vp, vp, sz, vp], i),
             "fk20_bench_field": ([i, i, vp, sz, i, vp], i),
             "fk20_version": ([], ctypes.c_char_p),
+            "fk20_ctx_profile": ([vp, i], i),
+            "fk20_ctx_profile_read": ([vp, i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long),
+                                       ctypes.POINTER(ctypes.c_double)], i),
+            "fk20_program_cost": ([i, ctypes.POINTER(i), ctypes.POINTER(i)], i),
+            "fk20_bench_imad": ([vp, i, i, i, vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -185,6 +194,18 @@ class Context:
 
     def device_bytes(self) -> int:
         return lib().fk20_ctx_device_bytes(self.h)
+
+    def profile(self, enable: bool = True):
+        call("fk20_ctx_profile", self.h, int(enable))
+
+    def profile_read(self) -> dict:
+        """{kind: (ms, launches, products)} accumulated since profile(True)."""
+        out = {}
+        for k, name in enumerate(KINDS):
+            ms, n, pr = ctypes.c_double(), ctypes.c_long(), ctypes.c_double()
+            call("fk20_ctx_profile_read", self.h, k, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(pr))
+            out[name] = (ms.value, n.value, pr.value)
+        return out
 
 
 def version() -> str:

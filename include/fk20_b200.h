@@ -96,6 +96,27 @@ int fk20_ctx_batch(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polys, unsigned coun
 /* Device bytes the context holds (tables + workspaces). */
 size_t fk20_ctx_device_bytes(const fk20_ctx *ctx);
 
+/* Per-launch profiling (no reference counterpart; the reference times whole
+ * calls with cudaEvents in fk20benchmark.cu:103-116).  While enabled, every
+ * pipeline kernel a call on this context launches is bracketed by CUDA events
+ * on its stream and tagged with its algorithmic work in 32x32->64-bit limb
+ * products.  fk20_ctx_profile(ctx, 1) resets the totals and enables;
+ * fk20_ctx_profile_read waits for the recorded launches and returns the totals
+ * of one kernel kind. */
+#define FK20_K_TC_FFT 0    /* toeplitz + Fr FFTs */
+#define FK20_K_MSM 1       /* fixed-base MSM */
+#define FK20_K_STAGE_INV 2 /* inverse G1 FFT stages */
+#define FK20_K_STAGE_FWD 3 /* forward G1 FFT stages */
+#define FK20_K_MIDDLE 4    /* last inverse + zeroing + first forward stage */
+#define FK20_K_OUTPUT 5    /* tiles -> reference g1p_t */
+#define FK20_NKINDS 6
+int fk20_ctx_profile(fk20_ctx *ctx, int enable);
+int fk20_ctx_profile_read(fk20_ctx *ctx, int kind, double *ms, long *launches, double *products);
+
+/* Doublings and additions of the fixed-scalar G1 program `index` (0..511:
+ * w_512^index; 512 + s: 2^-s), for work accounting. */
+int fk20_program_cost(int index, int *dbl, int *add);
+
 /* ------------------------------------------------------------------ reference entry points
  * These use a process-wide default context on the current device; tables are
  * rebuilt when the content of xext_fft changes (checked by a device-side
@@ -180,6 +201,11 @@ int g1a_fromG1p_n(g1a_t *a, const g1p_t *p, size_t count, void *stream);
  * 1 = Fr; sqr != 0 squares).  data: count x N 32-bit words, limb-major
  * (word k of element e at data[k * count + e]). */
 int fk20_bench_field(int field, int sqr, uint32_t *data, size_t count, int iters, void *stream);
+
+/* IMAD-pipe peak probe: blocks x threads threads, each running iters x 32
+ * independent 32-bit multiply-adds (8 chains); the caller times it.  The
+ * roofline denominator for this integer workload. */
+int fk20_bench_imad(uint32_t *sink, int blocks, int threads, int iters, void *stream);
 
 /* Engine version string. */
 const char *fk20_version(void);
