@@ -8,7 +8,7 @@
 // plain (non-Montgomery) values with Barrett reduction (fp.cuh:10-14,
 // fr.cuh:10-24, fr_mul.cu:58-186); conversion happens at the ABI boundary.
 //
-// Montgomery product: word-serial CIOS with the partial products of each
+// Montgomery product r = A*B/2^(32N): word-serial CIOS with the partial products of each
 // word b_i split between two accumulators, `e` (products a_j*b_i with j even:
 // lo at word j, hi at word j+1) and `o` (j odd).  Within one accumulator the
 // lo/hi words of different j never overlap, so each half is a single
@@ -16,9 +16,10 @@
 // reduction multiple m*p is split the same way.  After the reduction the
 // word-0 sum e0+o0 is 0 mod 2^32; its carry (0 or 1) is fed into the next
 // iteration at word 0 of the odd chain, and both accumulators shift down one
-// word.  Bounds: with inputs < 2p and 4p < 2^384 every partial value stays
-// below 2^416, so 13 words per accumulator suffice and the final value is
-// < 2p (one conditional subtraction of p makes it canonical).
+// word.  Bounds: with A < 2p (4p < 2^384) and B < 2^384 every partial value
+// stays below 2^416, so 13 words per accumulator suffice, and the result is
+// < 2p when A, B < 2p or when A < p (one conditional subtraction of p makes
+// it canonical).  A must not exceed ~2^382: a full-width A overflows.
 #pragma once
 #include "limbs.cuh"
 
@@ -257,13 +258,16 @@ FK_HD void f_cmov(Elem<F> &r, const Elem<F> &a, bool cond) {
     for (int i = 0; i < F::N; i++) r.w[i] = (a.w[i] & m) | (r.w[i] & ~m);
 }
 
-// standard form (any value < 2^(32N)) -> Montgomery form, canonical
+// standard form (any value < 2^(32N)) -> Montgomery form, canonical.  The
+// reduced constant R^2 mod m goes in the first (multiplicand) slot: f_mul's
+// accumulator bound needs that operand below ~2^(32N - 2), while the second
+// operand, scanned word by word, may be any 32N-bit value.
 template <class F>
 FK_HD void f_to_mont(Elem<F> &r, const Elem<F> &a) {
     Elem<F> r2;
 #pragma unroll
     for (int i = 0; i < F::N; i++) r2.w[i] = F::r2(i);
-    f_mul<F>(r, a, r2);
+    f_mul<F>(r, r2, a);
 }
 
 // Montgomery form -> canonical standard form
