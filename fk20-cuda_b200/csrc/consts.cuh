@@ -13,7 +13,8 @@ constexpr int MAX_LOG_M = 9;     // FFT sizes up to 512 (n = 4096, l = 16)
 constexpr int NPROG = 512 + 16;  // w_512^t for t < 512, then 2^-s at index 512 + s
 constexpr int L_COLS = 16;       // l: toeplitz columns per row (fk20_multi_cuda.py:328)
 
-static __constant__ uint32_t c_prog[NPROG][PROG_WORDS];
+// fixed-scalar programs: read with warp-uniform addresses (one broadcast per load)
+static __device__ uint32_t c_prog[NPROG][PROG_WORDS];
 static __device__ uint32_t g_fr_tw[512][8];   // w_512^t * 2^256 mod r (Montgomery form)
 static __device__ uint32_t g_fr_inv2[16][8];  // 2^-s * 2^256 mod r
 

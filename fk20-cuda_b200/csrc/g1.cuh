@@ -11,6 +11,29 @@
 
 namespace fk {
 
+// Fp products of the curve formulas.  A translation unit that defines
+// FK_FP_MUL_OUTLINE gets one out-of-line copy of the ~700-instruction product
+// that every call site shares (operands and result pass in registers): loops
+// over point operations then fit the instruction cache instead of streaming
+// hundreds of KB of inlined code.  Otherwise the product is inlined.
+#if defined(__CUDACC__) && defined(FK_FP_MUL_OUTLINE)
+static __device__ __noinline__ Fp fp_mul_outline(Fp a, Fp b) {
+    Fp r;
+    f_mul(r, a, b);
+    return r;
+}
+#endif
+
+FK_HD void fp_mul(Fp &r, const Fp &a, const Fp &b) {
+#if defined(__CUDA_ARCH__) && defined(FK_FP_MUL_OUTLINE)
+    r = fp_mul_outline(a, b);
+#else
+    f_mul(r, a, b);
+#endif
+}
+
+FK_HD void fp_sqr(Fp &r, const Fp &a) { fp_mul(r, a, a); }
+
 struct G1P {
     Fp x, y, z;
 };
@@ -69,31 +92,31 @@ template <class QT>
 FK_HD void g1_add_q(G1P &R, const G1P &P, const QT &Q, bool negQ) {
     Fp t0, t1, t2, t3, t4, X3, Y3, Z3, q;
     Q.get(0, q);
-    f_mul(t0, P.x, q);
+    fp_mul(t0, P.x, q);
     Q.get(1, q);
-    f_mul(t1, P.y, q);
+    fp_mul(t1, P.y, q);
     if (negQ) f_neg(t1, t1);
     Q.get(2, q);
-    f_mul(t2, P.z, q);
+    fp_mul(t2, P.z, q);
     f_add(t3, P.x, P.y);
     Q.get(0, q);
     Q.get(1, t4);
     if (negQ) f_sub(t4, q, t4); else f_add(t4, q, t4);
-    f_mul(t3, t3, t4);
+    fp_mul(t3, t3, t4);
     f_add(t4, t0, t1);
     f_sub(t3, t3, t4);
     f_add(t4, P.y, P.z);
     Q.get(2, q);
     Q.get(1, X3);
     if (negQ) f_sub(X3, q, X3); else f_add(X3, X3, q);
-    f_mul(t4, t4, X3);
+    fp_mul(t4, t4, X3);
     f_add(X3, t1, t2);
     f_sub(t4, t4, X3);
     f_add(X3, P.x, P.z);
     Q.get(0, q);
     Q.get(2, Y3);
     f_add(Y3, q, Y3);
-    f_mul(X3, X3, Y3);
+    fp_mul(X3, X3, Y3);
     f_add(Y3, t0, t2);
     f_sub(Y3, X3, Y3);
     f_add(X3, t0, t0);
@@ -102,14 +125,14 @@ FK_HD void g1_add_q(G1P &R, const G1P &P, const QT &Q, bool negQ) {
     f_add(Z3, t1, t2);
     f_sub(t1, t1, t2);
     f_mul12(Y3, Y3);
-    f_mul(X3, t4, Y3);
-    f_mul(t2, t3, t1);
+    fp_mul(X3, t4, Y3);
+    fp_mul(t2, t3, t1);
     f_sub(X3, t2, X3);
-    f_mul(Y3, Y3, t0);
-    f_mul(t1, t1, Z3);
+    fp_mul(Y3, Y3, t0);
+    fp_mul(t1, t1, Z3);
     f_add(Y3, t1, Y3);
-    f_mul(t0, t0, t3);
-    f_mul(Z3, Z3, t4);
+    fp_mul(t0, t0, t3);
+    fp_mul(Z3, Z3, t4);
     f_add(Z3, Z3, t0);
     R.x = X3;
     R.y = Y3;
@@ -122,16 +145,16 @@ FK_HD void g1_add(G1P &R, const G1P &P, const G1P &Q) { g1_add_q(R, P, RegPoint{
 // R = P + (qx, qy) with Q affine and not infinity (RCB Algorithm 8, 11 M + 2 m_3b)
 FK_HD void g1_madd(G1P &R, const G1P &P, const Fp &qx, const Fp &qy) {
     Fp t0, t1, t2, t3, t4, X3, Y3, Z3;
-    f_mul(t0, P.x, qx);
-    f_mul(t1, P.y, qy);
+    fp_mul(t0, P.x, qx);
+    fp_mul(t1, P.y, qy);
     f_add(t3, qx, qy);
     f_add(t4, P.x, P.y);
-    f_mul(t3, t3, t4);
+    fp_mul(t3, t3, t4);
     f_add(t4, t0, t1);
     f_sub(t3, t3, t4);
-    f_mul(t4, qy, P.z);
+    fp_mul(t4, qy, P.z);
     f_add(t4, t4, P.y);
-    f_mul(Y3, qx, P.z);
+    fp_mul(Y3, qx, P.z);
     f_add(Y3, Y3, P.x);
     f_add(X3, t0, t0);
     f_add(t0, X3, t0);
@@ -139,14 +162,14 @@ FK_HD void g1_madd(G1P &R, const G1P &P, const Fp &qx, const Fp &qy) {
     f_add(Z3, t1, t2);
     f_sub(t1, t1, t2);
     f_mul12(Y3, Y3);
-    f_mul(X3, t4, Y3);
-    f_mul(t2, t3, t1);
+    fp_mul(X3, t4, Y3);
+    fp_mul(t2, t3, t1);
     f_sub(X3, t2, X3);
-    f_mul(Y3, Y3, t0);
-    f_mul(t1, t1, Z3);
+    fp_mul(Y3, Y3, t0);
+    fp_mul(t1, t1, Z3);
     f_add(Y3, t1, Y3);
-    f_mul(t0, t0, t3);
-    f_mul(Z3, Z3, t4);
+    fp_mul(t0, t0, t3);
+    fp_mul(Z3, Z3, t4);
     f_add(Z3, Z3, t0);
     R.x = X3;
     R.y = Y3;
@@ -156,23 +179,23 @@ FK_HD void g1_madd(G1P &R, const G1P &P, const Fp &qx, const Fp &qy) {
 // R = 2P (RCB Algorithm 9, 6 M + 2 S + 1 m_3b)
 FK_HD void g1_dbl(G1P &R, const G1P &P) {
     Fp t0, t1, t2, X3, Y3, Z3;
-    f_sqr(t0, P.y);
+    fp_sqr(t0, P.y);
     f_add(Z3, t0, t0);
     f_add(Z3, Z3, Z3);
     f_add(Z3, Z3, Z3);
-    f_mul(t1, P.y, P.z);
-    f_sqr(t2, P.z);
+    fp_mul(t1, P.y, P.z);
+    fp_sqr(t2, P.z);
     f_mul12(t2, t2);
-    f_mul(X3, t2, Z3);
+    fp_mul(X3, t2, Z3);
     f_add(Y3, t0, t2);
-    f_mul(Z3, t1, Z3);
+    fp_mul(Z3, t1, Z3);
     f_add(t1, t2, t2);
     f_add(t2, t1, t2);
     f_sub(t0, t0, t2);
-    f_mul(Y3, t0, Y3);
+    fp_mul(Y3, t0, Y3);
     f_add(Y3, X3, Y3);
-    f_mul(t1, P.x, P.y);
-    f_mul(X3, t0, t1);
+    fp_mul(t1, P.x, P.y);
+    fp_mul(X3, t0, t1);
     f_add(X3, X3, X3);
     R.x = X3;
     R.y = Y3;
@@ -192,7 +215,7 @@ FK_HD void g1_phi(G1P &R, const G1P &P) {
     Fp beta;
 #pragma unroll
     for (int i = 0; i < 12; i++) beta.w[i] = beta_mont(i);
-    f_mul(R.x, P.x, beta);
+    fp_mul(R.x, P.x, beta);
     R.y = P.y;
     R.z = P.z;
 }

@@ -7,6 +7,14 @@
 // butterfly of one row (g1p_fft.cu:25-177), so a 256-bit double-and-add per
 // thread with divergent bits.  The two GLV base points of each thread live in
 // a conflict-free shared-memory slot (word k of thread t at [k][t]).
+// out-of-line Fp products for the stage kernels (see g1.cuh): their loops over
+// point operations would otherwise not fit the instruction cache
+#ifndef FK_FFT_OUTLINE
+#define FK_FFT_OUTLINE 1
+#endif
+#if FK_FFT_OUTLINE
+#define FK_FP_MUL_OUTLINE 1
+#endif
 #include "consts.cuh"
 #include "launch.h"
 #include "layout.cuh"
@@ -15,7 +23,7 @@ namespace fk {
 
 cudaError_t upload_consts_fft() { return upload_module_consts(); }
 
-constexpr int FFT_THREADS = 128;
+constexpr int FFT_THREADS = 64;
 // minimum resident blocks per SM requested from ptxas for the stage kernels
 // (caps registers at 65536 / (FFT_THREADS * FK_FFT_MINB))
 #ifndef FK_FFT_MINB
@@ -26,7 +34,7 @@ constexpr int FFT_THREADS = 128;
 // kind 1: DIT with forward twiddles (bit-reversed in, natural out).
 template <int KIND>
 __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__restrict__ D, int G, int log_m, int s) {
-    __shared__ uint32_t slots[72][FFT_THREADS];
+    __shared__ uint32_t slots[36 * PROG_SLOTS][FFT_THREADS];
     const int m = 1 << log_m;
     const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -46,7 +54,9 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__
     const int i0 = ((b / half) * 2 * half) + j, i1 = i0 + half;
     uint4 *p0 = D + tile_index(g, m, i0);
     uint4 *p1 = D + tile_index(g, m, i1);
-    const StridedPoint sP{&slots[0][threadIdx.x], FFT_THREADS}, sPhi{&slots[36][threadIdx.x], FFT_THREADS};
+    const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS}, {&slots[36][threadIdx.x], FFT_THREADS},
+                                           {&slots[72][threadIdx.x], FFT_THREADS}, {&slots[108][threadIdx.x], FFT_THREADS}};
+    const StridedPoint &sP = slot[0];
     if (KIND == 0) {
         // x = u + v, y = (u - v) * w^-t
         G1P u, x;
@@ -61,7 +71,7 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__
         g1_add_q(x, u, sP, true);
         if (tix != 0) {
             sP.put(x);
-            g1_mul_prog(x, sP, sPhi, c_prog[tix]);
+            g1_mul_prog(x, slot, c_prog[tix]);
         }
         tile_store(p1, lane, x);
     } else {
@@ -72,7 +82,7 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__
             tile_load(v, p1, lane);
             if (tix != 0) {
                 sP.put(v);
-                g1_mul_prog(v, sP, sPhi, c_prog[tix]);
+                g1_mul_prog(v, slot, c_prog[tix]);
             }
             sP.put(v);
         }
@@ -88,7 +98,7 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__
 // (2q, 2q+1) -> both = a + b, optionally times 2^-log_m
 template <bool SCALE>
 __global__ void __launch_bounds__(FFT_THREADS) k_g1_middle(uint4 *__restrict__ D, int G, int log_m) {
-    __shared__ uint32_t slots[SCALE ? 72 : 1][FFT_THREADS];
+    __shared__ uint32_t slots[SCALE ? 36 * PROG_SLOTS : 1][FFT_THREADS];
     const int m = 1 << log_m;
     const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -101,9 +111,12 @@ __global__ void __launch_bounds__(FFT_THREADS) k_g1_middle(uint4 *__restrict__ D
     tile_load(v, p1, lane);
     g1_add(x, u, v);
     if (SCALE) {
-        const StridedPoint sP{&slots[0][threadIdx.x], FFT_THREADS}, sPhi{&slots[SCALE ? 36 : 0][threadIdx.x], FFT_THREADS};
-        sP.put(x);
-        g1_mul_prog(x, sP, sPhi, c_prog[512 + log_m]);
+        const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS},
+                                               {&slots[SCALE ? 36 : 0][threadIdx.x], FFT_THREADS},
+                                               {&slots[SCALE ? 72 : 0][threadIdx.x], FFT_THREADS},
+                                               {&slots[SCALE ? 108 : 0][threadIdx.x], FFT_THREADS}};
+        slot[0].put(x);
+        g1_mul_prog(x, slot, c_prog[512 + log_m]);
     }
     tile_store(p0, lane, x);
     tile_store(p1, lane, x);
@@ -111,18 +124,19 @@ __global__ void __launch_bounds__(FFT_THREADS) k_g1_middle(uint4 *__restrict__ D
 
 // every point of the tiles times program `prog`
 __global__ void __launch_bounds__(FFT_THREADS) k_g1_scale(uint4 *__restrict__ D, int G, int log_m, int prog) {
-    __shared__ uint32_t slots[72][FFT_THREADS];
+    __shared__ uint32_t slots[36 * PROG_SLOTS][FFT_THREADS];
     const int m = 1 << log_m;
     const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     const int g = warp % G, i = warp / G;
     if (i >= m) return;
     uint4 *p = D + tile_index(g, m, i);
-    const StridedPoint sP{&slots[0][threadIdx.x], FFT_THREADS}, sPhi{&slots[36][threadIdx.x], FFT_THREADS};
+    const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS}, {&slots[36][threadIdx.x], FFT_THREADS},
+                                           {&slots[72][threadIdx.x], FFT_THREADS}, {&slots[108][threadIdx.x], FFT_THREADS}};
     G1P u;
     tile_load(u, p, lane);
-    sP.put(u);
-    g1_mul_prog(u, sP, sPhi, c_prog[prog]);
+    slot[0].put(u);
+    g1_mul_prog(u, slot, c_prog[prog]);
     tile_store(p, lane, u);
 }
 

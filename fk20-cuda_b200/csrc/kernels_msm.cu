@@ -9,6 +9,9 @@
 // (RCB Algorithm 8) of a gathered 96-byte entry: no doublings at all, against
 // ~255 doublings + ~128 additions per term in the reference's g1p_mul loop.
 // One warp per (column c, group of 32 rows); lanes are rows.
+#if defined(FK_MSM_OUTLINE) && FK_MSM_OUTLINE
+#define FK_FP_MUL_OUTLINE 1
+#endif
 #include "consts.cuh"
 #include "launch.h"
 #include "layout.cuh"

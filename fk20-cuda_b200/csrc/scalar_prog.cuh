@@ -1,4 +1,4 @@
-// scalar_prog.cuh -- fixed-scalar G1 multiplication programs (GLV + NAF).
+// scalar_prog.cuh -- fixed-scalar G1 multiplication programs (GLV + wNAF).
 //
 // Every G1 FFT butterfly multiplies a data-dependent point by a FIXED scalar,
 // a power of the 512th root of unity w = 5^((r-1)/512) (the table fr_roots,
@@ -7,86 +7,88 @@
 // with the GLV endomorphism of BLS12-381 G1: k = k1 + k2*lambda (mod r) with
 // lambda = z^2 - 1 ~ 2^128, r = lambda^2 + lambda + 1, so k2 = k div lambda and
 // k1 = k mod lambda are both < 2^128, and [k]P = [k1]P + [k2]phi(P) with
-// phi(x, y) = (beta x, y).  k1 and k2 are recoded in NAF and interleaved:
-// ~128 doublings and ~86 additions instead of ~254 and ~128.  The result is
-// the same group element for every P in the order-r subgroup (all FK20 data).
+// phi(x, y) = (beta x, y).  k1 and k2 are recoded in width-3 NAF (digits 0,
+// +-1, +-3; nonzero digits at least 3 apart) and processed jointly over the
+// precomputed P, 3P, phi(P), phi(3P): ~124 doublings and ~62 additions
+// instead of ~254 and ~128.  Of k and r - k the cheaper one is encoded (and
+// the result negated).  The result equals [k]P for every P in the order-r
+// subgroup -- all FK20 data.
 //
 // Program layout (PROG_WORDS uint32 words):
-//   word 0       : bits 0-7 top digit position (0..135), bit 8 = scalar is 0,
-//                  bit 9 = scalar is +-1, bit 10 = negate the result (the
-//                  program encodes r - k when that is cheaper)
-//   words 1..17  : 4 bits per digit position p (word 1 + p/8, nibble p%8):
-//                  bit0 k1-digit nonzero, bit1 k1-digit negative,
-//                  bit2 k2-digit nonzero, bit3 k2-digit negative
-// Warps run one program for 32 independent points, so every branch in the
+//   word 0      : bits 0-7 top digit position, bit 8 = scalar is 0,
+//                 bit 9 = scalar is +-1, bit 10 = negate the result
+//   words 1..34 : one byte per digit position p (word 1 + p/4, byte p%4):
+//                 bits 0-2 the k1 digit, bits 4-6 the k2 digit, each coded as
+//                 bit0 nonzero, bit1 negative, bit2 magnitude 3 (else 1)
+// A warp runs one program for 32 independent points, so every branch in the
 // executor is warp-uniform.
 #pragma once
 #include "g1.cuh"
 
 namespace fk {
 
-constexpr int PROG_WORDS = 18;
-constexpr int PROG_POSITIONS = 8 * (PROG_WORDS - 1);
+constexpr int PROG_POSITIONS = 136;
+constexpr int PROG_WORDS = 1 + PROG_POSITIONS / 4;
+constexpr int PROG_SLOTS = 4;  // P, 3P, phi(P), phi(3P)
 
 // acc = [k] P for the program of k (P in the prime-order subgroup).  P is
-// read from the strided slot sP; phi(P) is written to sPhi first.  Only the
+// read from slot[0]; slots 1..3 receive 3P, phi(P), phi(3P).  Only the
 // accumulator lives in registers.
 template <class ProgPtr>
-FK_HD void g1_mul_prog(G1P &acc, const StridedPoint &sP, const StridedPoint &sPhi, ProgPtr prog) {
+FK_HD void g1_mul_prog(G1P &acc, const StridedPoint *slot, ProgPtr prog) {
     const uint32_t hdr = prog[0];
     if (hdr & 0x100u) { g1_set_inf(acc); return; }
     const bool negate = (hdr & 0x400u) != 0;
     if (hdr & 0x200u) {
-        sP.load(acc);
+        slot[0].load(acc);
         if (negate) f_neg(acc.y, acc.y);
         return;
     }
     {
-        G1P phi;
-        sP.get(0, phi.x);
         Fp beta;
 #pragma unroll
         for (int i = 0; i < 12; i++) beta.w[i] = beta_mont(i);
-        f_mul(phi.x, phi.x, beta);
-        sP.get(1, phi.y);
-        sP.get(2, phi.z);
-        sPhi.put(phi);
+        // 3P = 2P + P, then phi(P), phi(3P)
+        slot[0].load(acc);
+        g1_dbl(acc, acc);
+        g1_add_q(acc, acc, slot[0], false);
+        slot[1].put(acc);
+        fp_mul(acc.x, acc.x, beta);
+        slot[3].put(acc);
+        slot[0].load(acc);
+        fp_mul(acc.x, acc.x, beta);
+        slot[2].put(acc);
     }
     const int top = (int)(hdr & 0xffu);
     bool started = false;
     for (int pos = top; pos >= 0; pos--) {
         if (started) g1_dbl(acc, acc);
-        const uint32_t nib = (prog[1 + (pos >> 3)] >> ((pos & 7) * 4)) & 0xfu;
-        if (nib & 1u) {
-            if (started) {
-                g1_add_q(acc, acc, sP, (nib & 2u) != 0);
-            } else {
-                sP.load(acc);
-                if (nib & 2u) f_neg(acc.y, acc.y);
+        const uint32_t byte = (prog[1 + (pos >> 2)] >> ((pos & 3) * 8)) & 0xffu;
+        for (int h = 0; h < 2; h++) {
+            const uint32_t d = (byte >> (4 * h)) & 7u;
+            if (d & 1u) {
+                const StridedPoint q = slot[2 * h + ((d >> 2) & 1u)];
+                if (started) {
+                    g1_add_q(acc, acc, q, (d & 2u) != 0);
+                } else {
+                    q.load(acc);
+                    if (d & 2u) f_neg(acc.y, acc.y);
+                }
+                started = true;
             }
-            started = true;
-        }
-        if (nib & 4u) {
-            if (started) {
-                g1_add_q(acc, acc, sPhi, (nib & 8u) != 0);
-            } else {
-                sPhi.load(acc);
-                if (nib & 8u) f_neg(acc.y, acc.y);
-            }
-            started = true;
         }
     }
     if (negate) f_neg(acc.y, acc.y);
 }
 
-// register-only convenience form (setup-time and element-wise kernels): uses
-// a local 72-word scratch as the two slots
+// register-only convenience form (setup-time and element-wise kernels): a
+// local scratch array stands in for the slots
 template <class ProgPtr>
 FK_HD void g1_mul_prog(G1P &R, const G1P &P, ProgPtr prog) {
-    uint32_t slots[72];
-    StridedPoint sP{slots, 1}, sPhi{slots + 36, 1};
-    sP.put(P);
-    g1_mul_prog(R, sP, sPhi, prog);
+    uint32_t mem[36 * PROG_SLOTS];
+    const StridedPoint slot[PROG_SLOTS] = {{mem, 1}, {mem + 36, 1}, {mem + 72, 1}, {mem + 108, 1}};
+    slot[0].put(P);
+    g1_mul_prog(R, slot, prog);
 }
 
 // ---------------------------------------------------------------- host side (host-only functions)
@@ -104,7 +106,6 @@ inline void divmod256(uint64_t q[4], uint64_t rem[4], const uint64_t a[4], const
     uint64_t r[4] = {0, 0, 0, 0};
     for (int i = 0; i < 4; i++) q[i] = 0;
     for (int bit = 255; bit >= 0; bit--) {
-        // r = (r << 1) | a_bit
         for (int i = 3; i > 0; i--) r[i] = (r[i] << 1) | (r[i - 1] >> 63);
         r[0] = (r[0] << 1) | ((a[bit / 64] >> (bit % 64)) & 1);
         if (cmp_words(r, d, 4) >= 0) {
@@ -120,20 +121,27 @@ inline void divmod256(uint64_t q[4], uint64_t rem[4], const uint64_t a[4], const
     for (int i = 0; i < 4; i++) rem[i] = r[i];
 }
 
-// NAF digits of a < 2^128 into d[0..PROG_POSITIONS); returns top position or -1
-inline int naf128(int8_t *d, unsigned __int128 k) {
+// width-3 NAF digits (0, +-1, +-3) of k < 2^128 into d[0..PROG_POSITIONS);
+// returns the top position or -1
+inline int wnaf3(int8_t *d, unsigned __int128 k) {
     int top = -1;
     for (int i = 0; i < PROG_POSITIONS; i++) d[i] = 0;
     for (int i = 0; k != 0; i++) {
         if (k & 1) {
-            int v = 2 - (int)(k & 3);  // +1 or -1
+            int v = (int)(k & 7);
+            if (v >= 4) v -= 8;
             d[i] = (int8_t)v;
-            if (v > 0) k -= 1; else k += 1;
+            if (v > 0) k -= (unsigned)v; else k += (unsigned)(-v);
             top = i;
         }
         k >>= 1;
     }
     return top;
+}
+
+inline uint32_t digit_code(int v) {
+    if (v == 0) return 0;
+    return 1u | (v < 0 ? 2u : 0u) | ((v == 3 || v == -3) ? 4u : 0u);
 }
 
 // program for a standard-form scalar k < r (4 x 64-bit words), no sign choice
@@ -149,18 +157,35 @@ inline void make_program_raw(uint32_t prog[PROG_WORDS], const uint64_t k[4]) {
     unsigned __int128 k1 = ((unsigned __int128)rem[1] << 64) | rem[0];
     unsigned __int128 k2 = ((unsigned __int128)q[1] << 64) | q[0];
     int8_t d1[PROG_POSITIONS], d2[PROG_POSITIONS];
-    int t1 = naf128(d1, k1), t2 = naf128(d2, k2);
+    int t1 = wnaf3(d1, k1), t2 = wnaf3(d2, k2);
     int top = t1 > t2 ? t1 : t2;
     prog[0] = (uint32_t)top;
     for (int p = 0; p <= top; p++) {
-        uint32_t nib = 0;
-        if (d1[p]) nib |= 1u | (d1[p] < 0 ? 2u : 0u);
-        if (d2[p]) nib |= 4u | (d2[p] < 0 ? 8u : 0u);
-        prog[1 + (p >> 3)] |= nib << ((p & 7) * 4);
+        const uint32_t byte = digit_code(d1[p]) | (digit_code(d2[p]) << 4);
+        prog[1 + (p >> 2)] |= byte << ((p & 3) * 8);
     }
 }
 
-inline void program_cost(const uint32_t prog[PROG_WORDS], int *dbl, int *add);
+// algorithmic cost of a program in doublings and additions (the 3P
+// precompute included: 1 doubling + 1 addition; the two phi products are not)
+inline void program_cost(const uint32_t prog[PROG_WORDS], int *dbl, int *add) {
+    *dbl = *add = 0;
+    if (prog[0] & 0x300u) return;
+    int top = (int)(prog[0] & 0xff);
+    bool started = false;
+    *dbl = 1;
+    *add = 1;
+    for (int p = top; p >= 0; p--) {
+        if (started) (*dbl)++;
+        const uint32_t byte = (prog[1 + (p >> 2)] >> ((p & 3) * 8)) & 0xff;
+        for (int h = 0; h < 2; h++) {
+            if ((byte >> (4 * h)) & 1) {
+                if (started) (*add)++;
+                started = true;
+            }
+        }
+    }
+}
 
 // program for k: the cheaper of k and (r - k) followed by a negation
 inline void make_program(uint32_t prog[PROG_WORDS], const uint64_t k[4]) {
@@ -183,20 +208,6 @@ inline void make_program(uint32_t prog[PROG_WORDS], const uint64_t k[4]) {
     if (8 * d1 + 12 * a1 < 8 * d0 + 12 * a0) {
         alt[0] |= 0x400u;
         for (int i = 0; i < PROG_WORDS; i++) prog[i] = alt[i];
-    }
-}
-
-// algorithmic cost of a program in RCB units: doublings and additions
-inline void program_cost(const uint32_t prog[PROG_WORDS], int *dbl, int *add) {
-    *dbl = *add = 0;
-    if (prog[0] & 0x300u) return;
-    int top = (int)(prog[0] & 0xff);
-    bool started = false;
-    for (int p = top; p >= 0; p--) {
-        if (started) (*dbl)++;
-        uint32_t nib = (prog[1 + (p >> 3)] >> ((p & 7) * 4)) & 0xf;
-        if (nib & 1) { if (started) (*add)++; started = true; }
-        if (nib & 4) { if (started) (*add)++; started = true; }
     }
 }
 

@@ -88,16 +88,16 @@ def test_g1_ops(engine, kats):
         exp = O.g1_op(op if op != "normalize" else "normalize", pts, qts if two else None)
         assert np.array_equal(got, exp), op
     scal = np.stack([O.int_to_limbs(int.from_bytes(rng.bytes(32), "little"), 4) for _ in range(len(pts))])
-    engine.call("g1p_op_n", engine.G1_OPS["mul"], engine._ptr(out), engine._ptr(dp), engine._ptr(engine.to_device(scal)),
-                len(pts), st)
+    dscal = engine.to_device(scal)
+    engine.call("g1p_op_n", engine.G1_OPS["mul"], engine._ptr(out), engine._ptr(dp), engine._ptr(dscal), len(pts), st)
     assert np.array_equal(O.g1_normalize(engine.to_host(out)), O.g1_op("mul", pts, scal))
     # is_point on valid points, a broken point and the ANYINF infinity
     bad = pts.copy()
     bad[3, 0] ^= np.uint64(1)
     import torch
     flags = torch.zeros(len(pts), dtype=torch.uint8, device="cuda")
-    engine.call("g1p_op_n", engine.G1_OPS["is_point"], None, engine._ptr(engine.to_device(bad)),
-                ctypes_ptr(flags), len(pts), st)
+    dbad = engine.to_device(bad)
+    engine.call("g1p_op_n", engine.G1_OPS["is_point"], None, engine._ptr(dbad), ctypes_ptr(flags), len(pts), st)
     f = flags.cpu().numpy()
     assert f[3] == 0 and f.sum() == len(pts) - 1
 
@@ -122,16 +122,17 @@ def test_eq_and_affine(engine):
         sc[r, 12:18] = O.int_to_limbs(7, 6)
     sc[5] = pts[6]
     eq = torch.zeros(len(pts), dtype=torch.uint8, device="cuda")
-    engine.call("g1p_eq_n", ctypes_ptr(eq), engine._ptr(engine.to_device(pts)), engine._ptr(engine.to_device(sc)),
-                len(pts), engine._stream())
+    # keep every device buffer referenced until the kernels that read it are enqueued
+    dpts, dsc = engine.to_device(pts), engine.to_device(sc)
+    engine.call("g1p_eq_n", ctypes_ptr(eq), engine._ptr(dpts), engine._ptr(dsc), len(pts), engine._stream())
     e = eq.cpu().numpy()
     assert e[5] == 0 and e.sum() == len(pts) - 1
     aff = engine.empty((len(pts), 12))
-    engine.call("g1a_fromG1p_n", engine._ptr(aff), engine._ptr(engine.to_device(sc)), len(pts), engine._stream())
+    engine.call("g1a_fromG1p_n", engine._ptr(aff), engine._ptr(dsc), len(pts), engine._stream())
     assert np.array_equal(engine.to_host(aff), O.g1_normalize(sc)[:, :12])
     a = O.ints_to_array([1, 2, R + 1, R - 1], 4)
     b = O.ints_to_array([1, 3, 1, 2 * R - 1], 4)
     eqr = torch.zeros(4, dtype=torch.uint8, device="cuda")
-    engine.call("fr_eq_n", ctypes_ptr(eqr), engine._ptr(engine.to_device(a)), engine._ptr(engine.to_device(b)), 4,
-                engine._stream())
+    da, db = engine.to_device(a), engine.to_device(b)
+    engine.call("fr_eq_n", ctypes_ptr(eqr), engine._ptr(da), engine._ptr(db), 4, engine._stream())
     assert eqr.cpu().numpy().tolist() == [1, 0, 1, 1]
