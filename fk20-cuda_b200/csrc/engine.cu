@@ -240,9 +240,15 @@ struct Profiler {
 struct fk20_ctx {
     int device = 0;
     int window = 10;
+    int sms = 148;
+    int fused_fft = 1;  // run the G1 FFT stages as one persistent launch
     std::mutex mu;
     Tables tab[3];  // log_m 7, 8, 9
     DevBuf S, D, D2, scratch, xext, offs, fp_dev;
+    // persistent-launch state: per-position readiness, task counter, error flag
+    DevBuf ready, sync;
+    unsigned epoch = 0;
+    int *err_host = nullptr;  // pinned copy of the device error flag
     Profiler prof;
 };
 
@@ -317,6 +323,42 @@ int run_hext_to_hfft(Profiler &pf, uint4 *D, int G, int rows, int log_m, int sca
         CKL();
     }
     return 0;
+}
+
+// the same sequence as one persistent launch (kernels_fft.cu k_g1_fused)
+int run_hext_to_hfft_fused(fk20_ctx *ctx, uint4 *D, int G, int rows, int log_m, cudaStream_t st) {
+    const int m = 1 << log_m;
+    const size_t ready_bytes = (size_t)G * m * sizeof(unsigned);
+    if (ctx->ready.bytes < ready_bytes) {
+        CKR(ctx->ready.reserve(ready_bytes));
+        CK(cudaMemsetAsync(ctx->ready.p, 0, ctx->ready.bytes, st));
+        ctx->epoch = 0;
+    }
+    CKR(ctx->sync.reserve(256));
+    if (++ctx->epoch >= (1u << 26)) {  // counters carry epoch * 64: restart before they wrap
+        CK(cudaMemsetAsync(ctx->ready.p, 0, ctx->ready.bytes, st));
+        ctx->epoch = 1;
+    }
+    unsigned *next = (unsigned *)ctx->sync.p;
+    int *err = (int *)((char *)ctx->sync.p + 128);
+    CK(cudaMemsetAsync(next, 0, sizeof(unsigned), st));
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    double prod = 0;
+    for (int s = 0; s < log_m - 1; s++) prod += stage_products(rows, log_m, s, 0) + stage_products(rows, log_m, s + 1, 1);
+    prod += (double)rows * (m / 2) * ADD_P;
+    ctx->prof.begin(FK20_K_FFT_FUSED, prod, st);
+    launch_g1_fused(D, (unsigned *)ctx->ready.p, next, err, ctx->epoch, G, log_m, ctx->sms, st);
+    ctx->prof.end(st);
+    CKL();
+    if (ctx->err_host) CK(cudaMemcpyAsync(ctx->err_host, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
+// the inverse + forward transforms of the pipeline, fused or stage by stage
+int run_pipeline_fft(fk20_ctx *ctx, uint4 *D, int G, int rows, int log_m, cudaStream_t st) {
+    if (ctx->err_host && *ctx->err_host) return FK20_ETIMEOUT;  // a previous fused launch gave up
+    if (ctx->fused_fft) return run_hext_to_hfft_fused(ctx, D, G, rows, log_m, st);
+    return run_hext_to_hfft(ctx->prof, D, G, rows, log_m, 0, st);
 }
 
 int output_launch(Profiler &pf, uint64_t *dst, const uint4 *D, const size_t *row_off, int rows, int log_m,
@@ -507,7 +549,35 @@ int fk20_ctx_create(fk20_ctx **out, int device, int window) {
     fk20_ctx *c = new fk20_ctx();
     c->device = device;
     c->window = window;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sms = prop.multiProcessorCount;
+    {
+        DeviceGuard dg(device);
+        if (cudaMallocHost(&c->err_host, sizeof(int)) == cudaSuccess) *c->err_host = 0;
+        else { cudaGetLastError(); c->err_host = nullptr; }
+    }
     *out = c;
+    return 0;
+}
+
+int fk20_ctx_set(fk20_ctx *ctx, int option, int value) {
+    if (!ctx) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    switch (option) {
+    case FK20_OPT_FUSED_FFT: ctx->fused_fft = value != 0; return 0;
+    default: return FK20_EINVAL;
+    }
+}
+
+int fk20_ctx_status(fk20_ctx *ctx) {
+    if (!ctx) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    CK(cudaDeviceSynchronize());
+    if (ctx->err_host && *ctx->err_host) {
+        *ctx->err_host = 0;
+        return FK20_ETIMEOUT;
+    }
     return 0;
 }
 
@@ -524,6 +594,9 @@ int fk20_ctx_destroy(fk20_ctx *ctx) {
         ctx->xext.release();
         ctx->offs.release();
         ctx->fp_dev.release();
+        ctx->ready.release();
+        ctx->sync.release();
+        if (ctx->err_host) cudaFreeHost(ctx->err_host);
     }
     delete ctx;
     return 0;
@@ -600,7 +673,7 @@ int fk20_ctx_poly2h_fft(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polynomial, uns
     cudaStream_t st = S_(stream);
     const int G = (int)((rows + 31) / 32);
     CKR(pipeline_to_hext(ctx, T, polynomial, nullptr, rows, 0, st));
-    CKR(run_hext_to_hfft(ctx->prof, (uint4 *)ctx->D.p, G, (int)rows, log_m, 0, st));
+    CKR(run_pipeline_fft(ctx, (uint4 *)ctx->D.p, G, (int)rows, log_m, st));
     CKR(output_launch(ctx->prof, (uint64_t *)h_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st));
     return 0;
 }
@@ -674,7 +747,7 @@ int fk20_ctx_batch(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polys, unsigned coun
         Tables *T = tables_for(ctx, gr.log_m);
         const int G = (int)((gr.rows + 31) / 32);
         CKR(pipeline_to_hext(ctx, T, polys, doffs + gr.first, gr.rows, 0, st));
-        CKR(run_hext_to_hfft(ctx->prof, (uint4 *)ctx->D.p, G, (int)gr.rows, gr.log_m, 0, st));
+        CKR(run_pipeline_fft(ctx, (uint4 *)ctx->D.p, G, (int)gr.rows, gr.log_m, st));
         CKR(output_launch(ctx->prof, (uint64_t *)h_fft, (const uint4 *)ctx->D.p, doffs + gr.first + gr.rows,
                           (int)gr.rows, gr.log_m, 0, st));
     }

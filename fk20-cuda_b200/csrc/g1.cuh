@@ -176,26 +176,29 @@ FK_HD void g1_madd(G1P &R, const G1P &P, const Fp &qx, const Fp &qy) {
     R.z = Z3;
 }
 
-// R = 2P (RCB Algorithm 9, 6 M + 2 S + 1 m_3b)
+// R = 2P (RCB Algorithm 9, 6 M + 2 S + 1 m_3b), with the products reordered
+// so that the inputs die early: at most 6 field temporaries are live at once
+// (the listed order keeps 8), which matters when the products are
+// out-of-line calls and every live value holds a register across them.
 FK_HD void g1_dbl(G1P &R, const G1P &P) {
-    Fp t0, t1, t2, X3, Y3, Z3;
-    fp_sqr(t0, P.y);
+    Fp t0, t1, t2, t3, X3, Y3, Z3;
+    fp_sqr(t0, P.y);         // Y^2
+    fp_mul(t3, P.x, P.y);    // XY
+    fp_mul(t1, P.y, P.z);    // YZ
+    fp_sqr(t2, P.z);         // Z^2
+    f_mul12(t2, t2);         // b3 Z^2
     f_add(Z3, t0, t0);
     f_add(Z3, Z3, Z3);
-    f_add(Z3, Z3, Z3);
-    fp_mul(t1, P.y, P.z);
-    fp_sqr(t2, P.z);
-    f_mul12(t2, t2);
+    f_add(Z3, Z3, Z3);       // 8 Y^2
     fp_mul(X3, t2, Z3);
+    fp_mul(Z3, t1, Z3);      // 8 Y^3 Z
     f_add(Y3, t0, t2);
-    fp_mul(Z3, t1, Z3);
     f_add(t1, t2, t2);
-    f_add(t2, t1, t2);
+    f_add(t2, t1, t2);       // 3 b3 Z^2
     f_sub(t0, t0, t2);
     fp_mul(Y3, t0, Y3);
     f_add(Y3, X3, Y3);
-    fp_mul(t1, P.x, P.y);
-    fp_mul(X3, t0, t1);
+    fp_mul(X3, t0, t3);
     f_add(X3, X3, X3);
     R.x = X3;
     R.y = Y3;

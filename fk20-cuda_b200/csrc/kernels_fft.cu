@@ -56,42 +56,209 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__
     uint4 *p1 = D + tile_index(g, m, i1);
     const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS}, {&slots[36][threadIdx.x], FFT_THREADS},
                                            {&slots[72][threadIdx.x], FFT_THREADS}, {&slots[108][threadIdx.x], FFT_THREADS}};
-    const StridedPoint &sP = slot[0];
+    // Points pass through the shared-memory slots so that only the accumulator
+    // of the current point operation is held in registers.
+    G1P acc;
     if (KIND == 0) {
         // x = u + v, y = (u - v) * w^-t
-        G1P u, x;
-        tile_load(u, p0, lane);
-        {
-            G1P v;
-            tile_load(v, p1, lane);
-            sP.put(v);
-        }
-        g1_add_q(x, u, sP, false);
-        tile_store(p0, lane, x);
-        g1_add_q(x, u, sP, true);
+        tile_to_slot(slot[0], p0, lane);
+        tile_to_slot(slot[1], p1, lane);
+        slot[0].load(acc);
+        g1_add_q(acc, acc, slot[1], false);
+        tile_store(p0, lane, acc);
+        slot[0].load(acc);
+        g1_add_q(acc, acc, slot[1], true);
         if (tix != 0) {
-            sP.put(x);
-            g1_mul_prog(x, slot, c_prog[tix]);
+            slot[0].put(acc);
+            g1_mul_prog(acc, slot, c_prog[tix]);
         }
-        tile_store(p1, lane, x);
+        tile_store(p1, lane, acc);
     } else {
         // v' = v * w^t, x = u + v', y = u - v'
-        G1P u, x;
-        {
-            G1P v;
-            tile_load(v, p1, lane);
-            if (tix != 0) {
-                sP.put(v);
-                g1_mul_prog(v, slot, c_prog[tix]);
-            }
-            sP.put(v);
+        tile_to_slot(slot[0], p1, lane);
+        if (tix != 0) {
+            g1_mul_prog(acc, slot, c_prog[tix]);
+            slot[0].put(acc);
         }
-        tile_load(u, p0, lane);
-        g1_add_q(x, u, sP, false);
-        tile_store(p0, lane, x);
-        g1_add_q(x, u, sP, true);
-        tile_store(p1, lane, x);
+        tile_to_slot(slot[1], p0, lane);
+        slot[1].load(acc);
+        g1_add_q(acc, acc, slot[0], false);
+        tile_store(p0, lane, acc);
+        slot[1].load(acc);
+        g1_add_q(acc, acc, slot[0], true);
+        tile_store(p1, lane, acc);
     }
+}
+
+// ------------------------------------------------------------------ fused stages
+// One persistent launch runs the whole hext -> h_fft sequence of the plain
+// pipeline: inverse DIF stages 0..L-2, the middle stage, forward DIT stages
+// 1..L-1, over G row groups.  Work is a stream of warp tasks (one butterfly
+// of 32 rows) taken in stage-major order from a global counter; a task waits
+// until the two positions it reads were written by the previous stage
+// (per-position counters ready[g][i] = epoch * 64 + stage + 1, published with
+// release semantics after the task's stores).  Every task only waits on tasks
+// handed out before it, which are held by running warps, so the wait always
+// ends; it is still bounded (FUSED_SPIN_LIMIT polls) and on expiry the kernel
+// records an error code and returns instead of hanging.  Tile data written by
+// other SMs is read through L2 (ld.cg) so no stale L1 line is used.
+constexpr unsigned FUSED_SPIN_LIMIT = 1u << 24;
+
+struct FusedArgs {
+    uint4 *D;
+    unsigned *ready;    // [G][m]
+    unsigned *next;     // task counter (zeroed before the launch)
+    int *err;           // 0 = ok, else 1000 + stage that timed out
+    unsigned epoch;     // distinct per launch, < 2^26
+    int G, log_m;
+};
+
+FK_D void tile_to_slot_cg(const StridedPoint &slot, const uint4 *base, int lane) {
+#pragma unroll
+    for (int q = 0; q < TILE_Q; q++) {
+        const uint4 v = __ldcg(base + q * 32 + lane);
+        slot.base[(4 * q) * slot.stride] = v.x;
+        slot.base[(4 * q + 1) * slot.stride] = v.y;
+        slot.base[(4 * q + 2) * slot.stride] = v.z;
+        slot.base[(4 * q + 3) * slot.stride] = v.w;
+    }
+}
+
+FK_D void tile_store_cg(uint4 *base, int lane, const G1P &p) {
+    uint32_t w[36];
+#pragma unroll
+    for (int k = 0; k < 12; k++) { w[k] = p.x.w[k]; w[12 + k] = p.y.w[k]; w[24 + k] = p.z.w[k]; }
+#pragma unroll
+    for (int q = 0; q < TILE_Q; q++) __stcg(base + q * 32 + lane, make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]));
+}
+
+FK_D unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+FK_D void st_release(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// lane 0 waits until ready[a] and ready[b] reach `need`; false on timeout
+FK_D bool wait_ready(const unsigned *ra, const unsigned *rb, unsigned need, int lane) {
+    int ok = 1;
+    if (lane == 0) {
+        unsigned spins = 0;
+        while (ld_acquire(ra) < need || ld_acquire(rb) < need) {
+            if (++spins >= FUSED_SPIN_LIMIT) { ok = 0; break; }
+            __nanosleep(64);
+        }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __threadfence();
+    return ok != 0;
+}
+
+__global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_fused(FusedArgs a) {
+    __shared__ uint32_t slots[36 * PROG_SLOTS][FFT_THREADS];
+    const int m = 1 << a.log_m, L = a.log_m;
+    const int lane = threadIdx.x & 31;
+    const int per_stage = a.G * (m >> 1);
+    const int nstages = 2 * L - 1;  // L-1 inverse, middle, L-1 forward
+    const unsigned base = a.epoch * 64u;
+    const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS}, {&slots[36][threadIdx.x], FFT_THREADS},
+                                           {&slots[72][threadIdx.x], FFT_THREADS}, {&slots[108][threadIdx.x], FFT_THREADS}};
+    for (;;) {
+        unsigned task = 0;
+        if (lane == 0) task = atomicAdd(a.next, 1u);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        if (task >= (unsigned)(per_stage * nstages)) return;
+        if (*(volatile int *)a.err) return;
+        const int S = (int)(task / per_stage), t = (int)(task % per_stage);
+        const int g = t % a.G, b = t / a.G;
+        int i0, i1, tix = 0, kind;
+        if (S < L - 1) {  // inverse DIF stage s = S
+            kind = 0;
+            const int half = m >> (S + 1), j = b & (half - 1);
+            i0 = (b / half) * 2 * half + j;
+            i1 = i0 + half;
+            tix = ((m - (j << S)) << (MAX_LOG_M - L)) & 511;
+        } else if (S == L - 1) {  // middle
+            kind = 2;
+            i0 = 2 * b;
+            i1 = 2 * b + 1;
+        } else {  // forward DIT stage s = S - L + 1
+            kind = 1;
+            const int s = S - L + 1, half = 1 << s, j = b & (half - 1);
+            i0 = (b / half) * 2 * half + j;
+            i1 = i0 + half;
+            tix = (j << (L - 1 - s)) << (MAX_LOG_M - L);
+        }
+        unsigned *r0 = a.ready + (size_t)g * m + i0, *r1 = a.ready + (size_t)g * m + i1;
+        if (S > 0 && !wait_ready(r0, r1, base + (unsigned)S, lane)) {
+            if (lane == 0) atomicCAS(a.err, 0, 1000 + S);
+            return;
+        }
+        uint4 *p0 = a.D + tile_index(g, m, i0);
+        uint4 *p1 = a.D + tile_index(g, m, i1);
+        G1P acc;
+        if (kind == 0) {
+            tile_to_slot_cg(slot[0], p0, lane);
+            tile_to_slot_cg(slot[1], p1, lane);
+            slot[0].load(acc);
+            g1_add_q(acc, acc, slot[1], false);
+            tile_store_cg(p0, lane, acc);
+            slot[0].load(acc);
+            g1_add_q(acc, acc, slot[1], true);
+            if (tix != 0) {
+                slot[0].put(acc);
+                g1_mul_prog(acc, slot, c_prog[tix]);
+            }
+            tile_store_cg(p1, lane, acc);
+        } else if (kind == 2) {
+            tile_to_slot_cg(slot[1], p1, lane);
+            tile_to_slot_cg(slot[0], p0, lane);
+            slot[0].load(acc);
+            g1_add_q(acc, acc, slot[1], false);
+            tile_store_cg(p0, lane, acc);
+            tile_store_cg(p1, lane, acc);
+        } else {
+            tile_to_slot_cg(slot[0], p1, lane);
+            if (tix != 0) {
+                g1_mul_prog(acc, slot, c_prog[tix]);
+                slot[0].put(acc);
+            }
+            tile_to_slot_cg(slot[1], p0, lane);
+            slot[1].load(acc);
+            g1_add_q(acc, acc, slot[0], false);
+            tile_store_cg(p0, lane, acc);
+            slot[1].load(acc);
+            g1_add_q(acc, acc, slot[0], true);
+            tile_store_cg(p1, lane, acc);
+        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) {
+            st_release(r0, base + (unsigned)S + 1u);
+            st_release(r1, base + (unsigned)S + 1u);
+        }
+    }
+}
+
+int fused_blocks_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_g1_fused, FFT_THREADS, 0) != cudaSuccess) return 0;
+    return n;
+}
+
+void launch_g1_fused(uint4 *D, unsigned *ready, unsigned *next, int *err, unsigned epoch, int G, int log_m,
+                     int sms, cudaStream_t st) {
+    FusedArgs a{D, ready, next, err, epoch, G, log_m};
+    int per_sm = fused_blocks_per_sm();
+    if (per_sm < 1) per_sm = 1;
+    const int tasks_warps = G * ((1 << log_m) / 2);
+    int blocks = sms * per_sm;
+    const int max_blocks = (tasks_warps + FFT_THREADS / 32 - 1) / (FFT_THREADS / 32);
+    if (blocks > max_blocks) blocks = max_blocks;
+    k_g1_fused<<<blocks, FFT_THREADS, 0, st>>>(a);
 }
 
 // last DIF stage + zeroing of the upper half + first DIT stage: pairs
@@ -106,10 +273,12 @@ __global__ void __launch_bounds__(FFT_THREADS) k_g1_middle(uint4 *__restrict__ D
     if (q >= (m >> 1)) return;
     uint4 *p0 = D + tile_index(g, m, 2 * q);
     uint4 *p1 = D + tile_index(g, m, 2 * q + 1);
-    G1P u, v, x;
-    tile_load(u, p0, lane);
-    tile_load(v, p1, lane);
-    g1_add(x, u, v);
+    __shared__ uint32_t vs[36][FFT_THREADS];
+    const StridedPoint sv{&vs[0][threadIdx.x], FFT_THREADS};
+    G1P x;
+    tile_to_slot(sv, p1, lane);
+    tile_load(x, p0, lane);
+    g1_add_q(x, x, sv, false);
     if (SCALE) {
         const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS},
                                                {&slots[SCALE ? 36 : 0][threadIdx.x], FFT_THREADS},
@@ -134,8 +303,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_g1_scale(uint4 *__restrict__ D,
     const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS}, {&slots[36][threadIdx.x], FFT_THREADS},
                                            {&slots[72][threadIdx.x], FFT_THREADS}, {&slots[108][threadIdx.x], FFT_THREADS}};
     G1P u;
-    tile_load(u, p, lane);
-    slot[0].put(u);
+    tile_to_slot(slot[0], p, lane);
     g1_mul_prog(u, slot, c_prog[prog]);
     tile_store(p, lane, u);
 }

@@ -33,6 +33,8 @@ void launch_msm(const MsmArgs &a, cudaStream_t st);
 // kernels_fft.cu
 void launch_g1_stage(uint4 *D, int G, int log_m, int s, int kind, cudaStream_t st);
 void launch_g1_middle(uint4 *D, int G, int log_m, int scale, cudaStream_t st);
+void launch_g1_fused(uint4 *D, unsigned *ready, unsigned *next, int *err, unsigned epoch, int G, int log_m,
+                     int sms, cudaStream_t st);
 void launch_g1_scale(uint4 *D, int G, int log_m, int prog, cudaStream_t st);
 void launch_ref_to_tile(uint4 *D, const uint64_t *src, int rows, int G, int log_m, int bitrev_in, int zero_upper,
                         cudaStream_t st);

@@ -45,6 +45,19 @@ FK_D void tile_store(uint4 *__restrict__ base, int lane, const G1P &p) {
     for (int q = 0; q < TILE_Q; q++) base[q * 32 + lane] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
 }
 
+// tile point -> strided slot (shared memory), one uint4 at a time, without
+// holding the whole point in registers
+FK_D void tile_to_slot(const StridedPoint &slot, const uint4 *__restrict__ base, int lane) {
+#pragma unroll
+    for (int q = 0; q < TILE_Q; q++) {
+        const uint4 v = base[q * 32 + lane];
+        slot.base[(4 * q) * slot.stride] = v.x;
+        slot.base[(4 * q + 1) * slot.stride] = v.y;
+        slot.base[(4 * q + 2) * slot.stride] = v.z;
+        slot.base[(4 * q + 3) * slot.stride] = v.w;
+    }
+}
+
 // reference g1p_t (18 x u64 standard form, any representative) -> Montgomery point.
 // Any (X, Y, 0) is the point at infinity (reference G1P_ANYINF, g1.cuh:14).
 FK_D void g1p_from_ref(G1P &p, const uint64_t *__restrict__ g) {

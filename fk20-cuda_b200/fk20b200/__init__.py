@@ -36,10 +36,13 @@ ABI_SYMBOLS = (
     "fr_fft", "fr_ift", "g1p_fft", "g1p_ift", "fr_fft_n", "g1p_fft_n", "fp_op_n", "fr_op_n",
     "g1p_op_n", "fr_eq_n", "g1p_eq_n", "g1a_fromG1p_n", "fk20_bench_field", "fk20_version",
     "fk20_ctx_profile", "fk20_ctx_profile_read", "fk20_program_cost", "fk20_bench_imad",
+    "fk20_ctx_set", "fk20_ctx_status",
 )
 
 # kernel kinds of the per-launch profiler (FK20_K_* in the header)
-KINDS = ("tc_fft", "msm", "stage_inv", "stage_fwd", "middle", "output")
+KINDS = ("tc_fft", "msm", "stage_inv", "stage_fwd", "middle", "output", "fft_fused")
+FK20_ETIMEOUT = 1005
+FK20_OPT_FUSED_FFT = 1
 
 
 class Fk20Error(RuntimeError):
@@ -103,6 +106,8 @@ def lib() -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.c_double)], i),
             "fk20_program_cost": ([i, ctypes.POINTER(i), ctypes.POINTER(i)], i),
             "fk20_bench_imad": ([vp, i, i, i, vp], i),
+            "fk20_ctx_set": ([vp, i, i], i),
+            "fk20_ctx_status": ([vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -191,6 +196,12 @@ class Context:
         po = (ctypes.c_size_t * cnt)(*poly_off)
         oo = (ctypes.c_size_t * cnt)(*out_off)
         call("fk20_ctx_batch", self.h, _ptr(h_fft), _ptr(polys), cnt, n_arr, po, oo, _stream())
+
+    def set(self, option: int, value: int):
+        call("fk20_ctx_set", self.h, option, value)
+
+    def status(self) -> int:
+        return lib().fk20_ctx_status(self.h)
 
     def device_bytes(self) -> int:
         return lib().fk20_ctx_device_bytes(self.h)

@@ -44,6 +44,7 @@ typedef struct { fp_t x, y, z; } g1p_t;
 #define FK20_ENOSETUP 1002 /* context has no tables for this polynomial length */
 #define FK20_ENOMEM 1003   /* device allocation failed */
 #define FK20_ENODEV 1004   /* no usable sm_100 device */
+#define FK20_ETIMEOUT 1005 /* a persistent launch gave up waiting (results invalid) */
 
 /* ------------------------------------------------------------------ context
  * A context owns, on one device, the fixed-base tables built from xext_fft
@@ -93,6 +94,18 @@ int fk20_ctx_msm(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *tc_fft, unsigned ro
 int fk20_ctx_batch(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polys, unsigned count, const unsigned *n,
                    const size_t *poly_off, const size_t *out_off, void *stream);
 
+/* Options.  FK20_OPT_FUSED_FFT (default 1): run the inverse and forward G1
+ * FFT stages of the pipeline as one persistent launch whose warps take
+ * butterfly tasks in stage order and wait (bounded) for their inputs, instead
+ * of one launch per stage. */
+#define FK20_OPT_FUSED_FFT 1
+int fk20_ctx_set(fk20_ctx *ctx, int option, int value);
+
+/* Waits for the context's queued work; returns FK20_ETIMEOUT if a persistent
+ * launch gave up waiting (its outputs are then invalid), else 0 or a CUDA
+ * error.  Bounded waits, not traps: the device context stays usable. */
+int fk20_ctx_status(fk20_ctx *ctx);
+
 /* Device bytes the context holds (tables + workspaces). */
 size_t fk20_ctx_device_bytes(const fk20_ctx *ctx);
 
@@ -109,7 +122,8 @@ size_t fk20_ctx_device_bytes(const fk20_ctx *ctx);
 #define FK20_K_STAGE_FWD 3 /* forward G1 FFT stages */
 #define FK20_K_MIDDLE 4    /* last inverse + zeroing + first forward stage */
 #define FK20_K_OUTPUT 5    /* tiles -> reference g1p_t */
-#define FK20_NKINDS 6
+#define FK20_K_FFT_FUSED 6 /* all G1 FFT stages in one persistent launch */
+#define FK20_NKINDS 7
 int fk20_ctx_profile(fk20_ctx *ctx, int enable);
 int fk20_ctx_profile_read(fk20_ctx *ctx, int kind, double *ms, long *launches, double *products);
 

@@ -217,3 +217,21 @@ def test_invalid_arguments_rejected(engine):
         c.poly2h_fft(h, p, 1, 4096)  # no tables loaded
     assert e.value.code == engine.FK20_ENOSETUP
     c.close()
+
+
+def test_fused_and_staged_fft_agree(engine):
+    """The persistent stage-fused G1 FFT launch and the launch-per-stage path
+    give the same proofs; the fused launch reports no timeout."""
+    n, rows, m = 4096, 70, 512
+    ctx = ctx_for(engine, n)
+    poly = engine.to_device(O.seeded_fr(123, rows * n).reshape(rows, n, 4))
+    a, b = engine.empty((rows, m, 18)), engine.empty((rows, m, 18))
+    ctx.set(engine.FK20_OPT_FUSED_FFT, 1)
+    ctx.poly2h_fft(a, poly, rows, n)
+    assert ctx.status() == 0
+    ctx.set(engine.FK20_OPT_FUSED_FFT, 0)
+    ctx.poly2h_fft(b, poly, rows, n)
+    ctx.set(engine.FK20_OPT_FUSED_FFT, 1)
+    assert ctx.status() == 0
+    import torch
+    assert torch.equal(a, b)
