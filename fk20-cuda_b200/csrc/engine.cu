@@ -113,6 +113,15 @@ int current_device_ready() {
     return ensure_device(dev);
 }
 
+}  // namespace
+
+namespace fk {
+// constant tables uploaded to the current device (used by noalloc.cu)
+int device_ready() { return current_device_ready(); }
+}  // namespace fk
+
+namespace {
+
 #define CK(x)                                  \
     do {                                       \
         cudaError_t e_ = (x);                  \

@@ -36,12 +36,13 @@ ABI_SYMBOLS = (
     "fr_fft", "fr_ift", "g1p_fft", "g1p_ift", "fr_fft_n", "g1p_fft_n", "fp_op_n", "fr_op_n",
     "g1p_op_n", "fr_eq_n", "g1p_eq_n", "g1a_fromG1p_n", "fk20_bench_field", "fk20_version",
     "fk20_ctx_profile", "fk20_ctx_profile_read", "fk20_program_cost", "fk20_bench_imad",
-    "fk20_ctx_set", "fk20_ctx_status",
+    "fk20_ctx_set", "fk20_ctx_status", "g1p_fft_noalloc",
 )
 
 # kernel kinds of the per-launch profiler (FK20_K_* in the header)
 KINDS = ("tc_fft", "msm", "stage_inv", "stage_fwd", "middle", "output", "fft_fused")
 FK20_ETIMEOUT = 1005
+FK20_ETOOBIG = 1006
 FK20_OPT_FUSED_FFT = 1
 
 
@@ -108,6 +109,7 @@ def lib() -> ctypes.CDLL:
             "fk20_bench_imad": ([vp, i, i, i, vp], i),
             "fk20_ctx_set": ([vp, i, i], i),
             "fk20_ctx_status": ([vp], i),
+            "g1p_fft_noalloc": ([vp, vp, u, u, i, vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

@@ -45,6 +45,7 @@ typedef struct { fp_t x, y, z; } g1p_t;
 #define FK20_ENOMEM 1003   /* device allocation failed */
 #define FK20_ENODEV 1004   /* no usable sm_100 device */
 #define FK20_ETIMEOUT 1005 /* a persistent launch gave up waiting (results invalid) */
+#define FK20_ETOOBIG 1006  /* request larger than the fixed scratch of a no-allocation entry point */
 
 /* ------------------------------------------------------------------ context
  * A context owns, on one device, the fixed-base tables built from xext_fft
@@ -189,6 +190,17 @@ int g1p_ift(g1p_t *output, const g1p_t *input, unsigned count, void *stream);
 /* Size-generic transforms: log_m in 1..9. */
 int fr_fft_n(fr_t *output, const fr_t *input, unsigned log_m, unsigned count, int inverse, void *stream);
 int g1p_fft_n(g1p_t *output, const g1p_t *input, unsigned log_m, unsigned count, int inverse, void *stream);
+
+/* No counterpart in the reference.  The same transforms as g1p_fft_n for
+ * callers that must not have the library allocate device memory (their
+ * memory is owned by their own allocator or pool, or they cannot take the
+ * device-wide synchronisation of cudaMalloc/cudaFree): the working tiles live
+ * in a fixed file-scope device array of ~4.7 MB that every GPU loading the
+ * library holds until exit.  At most 64 transforms (log_m <= 9) per call;
+ * more returns FK20_ETOOBIG.  The first call on a device looks up the array's
+ * address and should come before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised. */
+int g1p_fft_noalloc(g1p_t *output, const g1p_t *input, unsigned log_m, unsigned count, int inverse, void *stream);
 
 /* ------------------------------------------------------------------ element-wise helpers
  * Batched forms of the fp_* / fr_* / g1p_* device API (fp.cuh:16-41,
