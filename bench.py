@@ -51,6 +51,15 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=0, help="rows per CPU sample (default: one per core)")
+    ap.add_argument("--mode", choices=("batch", "serve", "ragged", "micro"), default="batch",
+                    help="batch: the headline 512 x 4096 batch; serve: Poisson request load through the "
+                         "continuous-batching server; ragged: 1000 mixed-length instances as one graph-captured batch; "
+                         "micro: kernel microbenchmarks (Fp/Fr products, batched G1 FFT/IFFT, 16-term MSM)")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="arrival window per load level (serve)")
+    ap.add_argument("--serve-loads", default="0.5,0.9,1.2", help="offered load as fractions of plain-batch capacity")
+    ap.add_argument("--serve-max-rows", type=int, default=128)
+    ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--autotune", action="store_true", help="ragged: autotune the context first")
     return ap.parse_args()
 
 
@@ -337,6 +346,349 @@ def run_ours(args, ws, rank, dev):
     return line
 
 
+# ------------------------------------------------------------------ served load
+SERVE_MIX = ((1024, 0.2), (2048, 0.3), (4096, 0.5))
+
+
+def run_serve(args, ws, rank, dev):
+    """Open-loop Poisson arrivals of blob-proof requests (1024/2048/4096
+    coefficients, weights 0.2/0.3/0.5) at fractions of the measured plain-batch
+    capacity, through the continuous-batching server (fk20_server_*); p50/p99
+    latency (submit -> proofs in host memory) and sustained proofs/s beside the
+    plain 512 x 4096 batch."""
+    import queue
+    import threading
+    import numpy as np
+    import torch
+    import fk20b200 as E
+
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    ctx = E.Context(dev, args.window)
+    for n, _ in SERVE_MIX:
+        ctx.load_setup(n, gpu_setup(E, n))
+    torch.cuda.synchronize()
+    setup_s = time.time() - t0
+    # plain-batch capacity and latency: the full 512 x 4096 batch, device resident
+    rows, n = args.rows, args.n
+    poly = E.to_device(seeded_polys(1000 + rank, rows, n))
+    h = E.empty((rows, 2 * n // L, 18))
+    for _ in range(2):
+        ctx.poly2h_fft(h, poly, rows, n)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(3):
+        ctx.poly2h_fft(h, poly, rows, n)
+    e.record()
+    e.synchronize()
+    plain_ms = s.elapsed_time(e) / 3
+    plain_pps = rows * (2 * n // L) / (plain_ms * 1e-3)
+    del poly, h
+    # request pool: seeded polynomials per length, reused round-robin
+    pool = {n: [np.ascontiguousarray(p) for p in seeded_polys(5000 + n, 24, n)] for n, _ in SERVE_MIX}
+    sizes = np.array([n for n, _ in SERVE_MIX])
+    weights = np.array([w for _, w in SERVE_MIX])
+    mean_proofs = float((sizes // 8 * weights).sum())
+    srv = E.Server(ctx, max_rows=args.serve_max_rows, slots=args.serve_slots)
+    loads = []
+    rng = np.random.default_rng(42)
+    check = []  # (n, pool index, output) kept for the bit-exactness check
+    for frac in [float(x) for x in args.serve_loads.split(",")]:
+        rate = frac * plain_pps / mean_proofs  # requests per second
+        count = max(1, int(rate * args.serve_seconds))
+        gaps = rng.exponential(1.0 / rate, count)
+        lens = rng.choice(sizes, count, p=weights)
+        free = {int(n): [] for n in sizes}
+        pending = queue.Queue()
+        done_rc = []
+
+        def collector():
+            while True:
+                item = pending.get()
+                if item is None:
+                    return
+                t, n, j, out = item
+                done_rc.append(srv.wait(t, 120000))
+                if len(check) < 24 and j % 5 == 0:
+                    check.append((n, j % 24, out))
+                else:
+                    free[n].append(out)
+
+        th = threading.Thread(target=collector)
+        th.start()
+        srv.reset_stats()
+        start = time.perf_counter()
+        due = start
+        for j in range(count):
+            due += gaps[j]
+            d = due - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            n = int(lens[j])
+            out = free[n].pop() if free[n] else np.zeros((n // 8, 18), np.uint64)
+            t = srv.submit(pool[n][j % 24], out)
+            pending.put((t, n, j, out))
+        pending.put(None)
+        th.join()
+        st = srv.stats()
+        loads.append({"load": frac, "requests": count, "offered_proofs_per_s": rate * mean_proofs,
+                      "served_proofs_per_s": st["proofs_per_s"],
+                      "served_vs_plain": st["proofs_per_s"] / plain_pps,
+                      "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                      "max_ms": st["max_ms"], "p99_below_plain_batch_latency": st["p99_ms"] < plain_ms,
+                      "mean_pack_rows": st["mean_pack_rows"], "packs": st["packs"],
+                      "errors": sum(1 for r in done_rc if r != 0)})
+    srv.close()
+    # served results are the ones the same polynomial gives alone
+    same = True
+    for n, j, out in check:
+        hh = E.empty((1, n // 8, 18))
+        ctx.poly2h_fft(hh, E.to_device(pool[n][j].reshape(1, n, 4)), 1, n)
+        same &= bool(np.array_equal(E.to_host(hh)[0], out))
+    sat = max(loads, key=lambda x: x["load"])
+    line = {
+        "metric": "served KZG proofs/s, mixed 1024/2048/4096 requests, bit-exact; p50/p99 latency",
+        "value": sat["served_proofs_per_s"], "unit": "proofs/s", "n_gpus": ws, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "mode": "serve",
+        "data": "synthetic (seeded uniform Fr, seeded tau), open-loop Poisson arrivals",
+        "config": {"workload": "served load: Poisson arrivals of 1024/2048/4096-coefficient requests "
+                               "(weights 0.2/0.3/0.5) at fractions of plain-batch capacity",
+                   "window_bits": args.window, "max_rows_per_pack": args.serve_max_rows,
+                   "slots": args.serve_slots, "arrival_window_s": args.serve_seconds, "setup_s": round(setup_s, 2),
+                   "table_bytes": ctx.device_bytes()},
+        "plain_batch": {"rows": rows, "n": n, "proofs_per_s": plain_pps, "latency_ms": plain_ms},
+        "loads": loads, "results_same_alone_and_served": same, "checked_requests": len(check),
+        "impl": "ours",
+    }
+    ctx.close()
+    return line
+
+
+# ------------------------------------------------------------------ ragged batch (graph)
+def run_ragged(args, ws, rank, dev):
+    """1000 FK20 instances, lengths uniform over {1024, 2048, 4096}, one shared
+    setup: one ragged batch (one MSM launch + one persistent G1 FFT launch over
+    the three lengths) captured once in a CUDA graph and replayed; checked
+    against the plain per-length path."""
+    import numpy as np
+    import torch
+    import fk20b200 as E
+
+    torch.cuda.set_device(dev)
+    ctx = E.Context(dev, args.window)
+    for n in (1024, 2048, 4096):
+        ctx.load_setup(n, gpu_setup(E, n))
+    rng = np.random.default_rng(77 + rank)
+    sizes = [int(x) for x in rng.choice([1024, 2048, 4096], 1000)]
+    poly_off, out_off, po, oo = [], [], 0, 0
+    for n in sizes:
+        poly_off.append(po)
+        out_off.append(oo)
+        po += n
+        oo += n // 8
+    import oracle as O
+    polys = E.to_device(O.seeded_fr(31 + rank, po))
+    out = E.empty((oo, 18))
+    tune = None
+    if args.autotune:
+        tune = ctx.autotune(4096, rows=128, max_table_bytes=0)
+    plan = E.Plan(ctx, out, polys, sizes, poly_off, out_off)
+    for _ in range(args.warmup):
+        plan.launch()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    barrier(ws)
+    ms = []
+    stream = torch.cuda.current_stream()
+    for _ in range(args.steps):
+        flush.fill_(1)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        plan.launch()
+        e.record(stream)
+        e.synchronize()
+        ms.append(s.elapsed_time(e))
+    barrier(ws)
+    total = max_over_ranks(sum(ms), ws)
+    # direct (non-graph) call and the per-length plain path give the same proofs
+    direct = E.empty((oo, 18))
+    ctx.batch(direct, polys, sizes, poly_off, out_off)
+    exp = E.empty((oo, 18))
+    for n in (1024, 2048, 4096):
+        idx = [j for j, s_ in enumerate(sizes) if s_ == n]
+        rows = torch.stack([polys[poly_off[j]:poly_off[j] + n] for j in idx])
+        h = E.empty((len(idx), n // 8, 18))
+        ctx.poly2h_fft(h, rows, len(idx), n)
+        for r, j in enumerate(idx):
+            exp[out_off[j]:out_off[j] + n // 8] = h[r]
+    torch.cuda.synchronize()
+    proofs = oo
+    line = {
+        "metric": "KZG proofs/s, ragged batch of 1000 instances (1024/2048/4096), bit-exact",
+        "value": ws * proofs * args.steps / (total * 1e-3), "unit": "proofs/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "mode": "ragged",
+        "data": "synthetic (seeded uniform Fr, seeded tau)",
+        "config": {"workload": "1000 FK20 instances, lengths uniform over {1024, 2048, 4096}, one CUDA-graph "
+                               "replay per step", "window_bits": args.window, "proofs_per_step": proofs,
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "graph_equals_direct": bool(torch.equal(out, direct)), "equals_per_length_path": bool(torch.equal(out, exp)),
+        "autotune": tune, "impl": "ours",
+    }
+    plan.close()
+    ctx.close()
+    return line
+
+
+# ------------------------------------------------------------------ kernel microbenchmarks
+MP, MR = 300, 136  # limb products per Fp / Fr Montgomery product
+
+
+def _timed(fn, reps, stream):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(reps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        fn()
+        e.record(stream)
+        e.synchronize()
+        t = s.elapsed_time(e)
+        best = t if best is None else min(best, t)
+    return best
+
+
+def run_micro(args, ws, rank, dev):
+    """2^24 independent Fp and Fr Montgomery products and squarings on uniform
+    seeded residues; 512-point G1 FFT and IFFT over 512 rows of seeded
+    multiples of G1; the 512 x 16-term fixed-base MSM with uniform scalars.
+    Each output is checked bit-exact on a sample against the oracle; each
+    kernel is reported against the IMAD roofline (limb products/s over the
+    measured IMAD peak / 2)."""
+    import numpy as np
+    import torch
+    import fk20b200 as E
+    import oracle as O
+
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    peak = measure_imad_peak(E, torch) / 2
+    out = {}
+    # ---- field products: limb-major Montgomery data, `iters` dependent products per element
+    count, iters = 1 << 24, 64
+    rng = np.random.default_rng(3)
+    for field, mod, nl, mp in (("fp", O.P, 12, MP), ("fr", O.R, 8, MR)):
+        words = rng.integers(0, 2**32, (nl, count), dtype=np.uint64).astype(np.uint32)
+        words[nl - 1] &= np.uint32((1 << (mod.bit_length() - 32 * (nl - 1) - 1)) - 1)  # < 2^(bits-1) < mod
+        d0 = torch.from_numpy(words.view(np.int32)).cuda()
+        for sq in (0, 1):
+            d = d0.clone()
+            ms = _timed(lambda: E.call("fk20_bench_field", 0 if field == "fp" else 1, sq, E._ptr(d), count, iters,
+                                       E._stream()), 3, stream)
+            # bit-exactness on a sample: one more run from the same input, against pow() over the integers
+            d = d0.clone()
+            E.call("fk20_bench_field", 0 if field == "fp" else 1, sq, E._ptr(d), count, iters, E._stream())
+            got = d.cpu().numpy().view(np.uint32)
+            Rm = pow(2, 32 * nl, mod)
+            Ri = pow(Rm, mod - 2, mod)
+            ok = True
+            for e in range(0, count, count // 16):
+                X = sum(int(words[k, e]) << (32 * k) for k in range(nl))
+                x = X * Ri % mod
+                y = pow(x, 2 ** iters, mod) if sq else pow(x, iters + 1, mod)
+                G = sum(int(got[k, e]) << (32 * k) for k in range(nl))
+                ok &= G == y * Rm % mod
+            prod = count * iters * mp
+            out[f"{field}_{'sqr' if sq else 'mul'}"] = {
+                "elements": count, "products_per_element": iters, "ms": ms,
+                "gmul_per_s": count * iters / (ms * 1e-3) / 1e9,
+                "achieved_gprod_s": prod / (ms * 1e-3) / 1e9, "frac": prod / (ms * 1e-3) / peak, "bit_exact_sample": ok}
+    # ---- G1 FFT / IFFT, 512 rows x 512 points
+    rows, m = 512, 512
+    gen = E.to_device(np.repeat(O.g1_generator().reshape(1, 18), rows * m, 0))
+    scal = E.to_device(O.seeded_fr(21, rows * m))
+    pts = E.empty((rows, m, 18))
+    E.call("g1p_op_n", E.G1_OPS["mul"], E._ptr(pts), E._ptr(gen), E._ptr(scal), rows * m, E._stream())
+    del gen, scal
+    res = E.empty((rows, m, 18))
+    costs = [E.program_cost(i) for i in range(512 + 10)]
+
+    def prog_products(idx):
+        dbl, add = costs[idx]
+        return (dbl * 8 + add * 12 + 1) * MP if dbl or add else 0.0
+
+    def fft_products(inverse):
+        tot = 0.0
+        log_m = 9
+        for st_ in range(log_m):
+            for b in range(m // 2):
+                if inverse:
+                    half = m >> (st_ + 1)
+                    j = b & (half - 1)
+                    tix = (m - (j << st_)) & 511
+                else:
+                    half = 1 << st_
+                    j = b & (half - 1)
+                    tix = j << (log_m - 1 - st_)
+                tot += 2 * 12 * MP
+                if tix:
+                    tot += prog_products(tix)
+        if inverse:  # times 2^-9 on every point
+            tot += m * prog_products(512 + 9)
+        return tot * rows
+
+    for name, inv in (("g1_fft", 0), ("g1_ift", 1)):
+        ms = _timed(lambda: E.call("g1p_fft_n", E._ptr(res), E._ptr(pts), 9, rows, inv, E._stream()), 3, stream)
+        host_in = E.to_host(pts[:2])
+        exp = O.g1_fft(host_in, inverse=bool(inv))
+        got = O.g1_normalize(E.to_host(res[:2]).reshape(-1, 18)).reshape(exp.shape)
+        prod = fft_products(inv)
+        out[name] = {"rows": rows, "m": m, "ms": ms, "achieved_gprod_s": prod / (ms * 1e-3) / 1e9,
+                     "frac": prod / (ms * 1e-3) / peak, "bit_exact_sample_rows": 2,
+                     "bit_exact": bool(np.array_equal(got, exp))}
+    del pts, res
+    # ---- 16-term fixed-base MSM: tc_fft[512][16][512] uniform Fr -> hext_fft[512][512]
+    n = 4096
+    setup = gpu_setup(E, n)
+    xext = E.empty((L, m, 18))
+    E.call("fk20_setup2xext_fft", E._ptr(xext), E._ptr(setup), E._stream())
+    ctx = E.Context(dev, args.window)
+    ctx.load_xext_fft(n, xext)
+    tc = O.seeded_fr(22, rows * L * m).reshape(rows, L, m, 4)
+    dtc = E.to_device(tc)
+    hext = E.empty((rows, m, 18))
+    ctx.profile(True)
+    ms = _timed(lambda: ctx.msm(hext, dtc, rows, n), 3, stream)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    kms, kl, kprod = prof["msm"]
+    xh = E.to_host(xext)
+    got = O.g1_normalize(E.to_host(hext[:, :4]).reshape(-1, 18)).reshape(rows, 4, 18)
+    ok = True
+    for r in (0, rows - 1):
+        for c in range(4):
+            acc = None
+            terms = O.g1_op("mul", xh[:, c], np.ascontiguousarray(tc[r, :, c]))
+            acc = terms[0:1]
+            for i in range(1, L):
+                acc = O.g1_op("add", acc, terms[i:i + 1])
+            ok &= bool(np.array_equal(O.g1_normalize(acc)[0], got[r, c]))
+    out["msm"] = {"rows": rows, "columns": m, "terms": L, "window_bits": args.window, "ms": ms,
+                  "kernel_ms": kms / kl, "achieved_gprod_s": kprod / kl / (kms / kl * 1e-3) / 1e9,
+                  "frac": kprod / kl / (kms / kl * 1e-3) / peak, "bit_exact_sample": ok}
+    ctx.close()
+    line = {"metric": "kernel microbenchmarks: fraction of the IMAD roofline, bit-exact samples",
+            "value": min(v["frac"] for v in out.values()), "unit": "min frac of IMAD roofline",
+            "n_gpus": ws, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "mode": "micro", "data": "synthetic (seeded uniform residues, seeded multiples of G1)",
+            "config": {"workload": "2^24 Fp/Fr mul and sqr; 512 x 512-point G1 FFT/IFFT; 512 x 16-term MSM",
+                       "imad_peak_gprod_s": peak / 1e9}, "kernels": out, "impl": "ours"}
+    return line
+
+
 # ------------------------------------------------------------------ reference arm
 def run_reference(args, ws, rank):
     """The reference's CPU path for this workload -- FK20Py multi
@@ -386,7 +738,14 @@ def main():
             print(json.dumps(run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), rank)), flush=True)
         return
     ws, rank, local = dist_init(args)
-    line = run_ours(args, ws, rank, local)
+    if args.mode == "serve":
+        line = run_serve(args, ws, rank, local)
+    elif args.mode == "ragged":
+        line = run_ragged(args, ws, rank, local)
+    elif args.mode == "micro":
+        line = run_micro(args, ws, rank, local)
+    else:
+        line = run_ours(args, ws, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -11,10 +11,17 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/fk20_b200.h"
@@ -183,7 +190,64 @@ struct Tables {
     unsigned n = 0;
     int log_m = 0, cb = 0, W = 0;
     DevBuf table;
+    DevBuf xext;             // the xext_fft the tables were built from (rebuilds at another window)
+    unsigned gen = 0;        // bumped at every build: graph plans check it before replaying
     unsigned long long fingerprint = 0;
+};
+
+// Device state of one in-flight pipeline call: scalar and point tiles, the
+// offset arrays of ragged batches, and the persistent launch's counters.  A
+// context owns one; every batch plan and server slot owns its own, so that
+// they can run on different streams at once against the same tables.
+struct Workspace {
+    DevBuf S, D, offs, sync;           // sync: [task counter | error flag | pad][readiness counters]
+    int *err_host = nullptr;           // pinned copy of the last persistent launch's error flag
+    size_t *offs_host = nullptr;       // pinned staging of offset arrays
+    size_t offs_cap = 0;               // entries of offs_host
+    cudaEvent_t offs_done = nullptr;   // the last copy out of offs_host
+    int init() {
+        if (err_host) return 0;
+        if (cudaMallocHost(&err_host, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            err_host = nullptr;
+            return FK20_ENOMEM;
+        }
+        *err_host = 0;
+        return 0;
+    }
+    // pinned staging for `count` offsets with no copy out of it pending
+    int stage_offsets(size_t count) {
+        if (offs_done) {
+            CK(cudaEventSynchronize(offs_done));
+        } else {
+            CK(cudaEventCreateWithFlags(&offs_done, cudaEventDisableTiming));
+        }
+        if (count > offs_cap) {
+            if (offs_host) cudaFreeHost(offs_host);
+            offs_host = nullptr;
+            offs_cap = 0;
+            if (cudaMallocHost(&offs_host, count * sizeof(size_t)) != cudaSuccess) {
+                cudaGetLastError();
+                return FK20_ENOMEM;
+            }
+            offs_cap = count;
+        }
+        return 0;
+    }
+    size_t bytes() const { return S.bytes + D.bytes + offs.bytes + sync.bytes; }
+    void release() {
+        S.release();
+        D.release();
+        offs.release();
+        sync.release();
+        if (err_host) cudaFreeHost(err_host);
+        if (offs_host) cudaFreeHost(offs_host);
+        if (offs_done) cudaEventDestroy(offs_done);
+        err_host = nullptr;
+        offs_host = nullptr;
+        offs_cap = 0;
+        offs_done = nullptr;
+    }
 };
 
 }  // namespace
@@ -250,14 +314,14 @@ struct fk20_ctx {
     int device = 0;
     int window = 10;
     int sms = 148;
-    int fused_fft = 1;  // run the G1 FFT stages as one persistent launch
+    int fused_fft = 1;          // run the G1 FFT stages as one persistent launch
+    int msm_threads = 128;      // MSM block size (64, 128, 256)
+    int fft_blocks_per_sm = 0;  // persistent FFT grid: blocks per SM (0 = as many as fit)
+    int fused_occupancy = 1;    // blocks of the persistent FFT kernel that fit on one SM
     std::mutex mu;
     Tables tab[3];  // log_m 7, 8, 9
-    DevBuf S, D, D2, scratch, xext, offs, fp_dev;
-    // persistent-launch state: per-position readiness, task counter, error flag
-    DevBuf ready, sync;
-    unsigned epoch = 0;
-    int *err_host = nullptr;  // pinned copy of the device error flag
+    Workspace ws;   // the context's own calls
+    DevBuf D2, scratch, xext, fp_dev;
     Profiler prof;
 };
 
@@ -334,42 +398,6 @@ int run_hext_to_hfft(Profiler &pf, uint4 *D, int G, int rows, int log_m, int sca
     return 0;
 }
 
-// the same sequence as one persistent launch (kernels_fft.cu k_g1_fused)
-int run_hext_to_hfft_fused(fk20_ctx *ctx, uint4 *D, int G, int rows, int log_m, cudaStream_t st) {
-    const int m = 1 << log_m;
-    const size_t ready_bytes = (size_t)G * m * sizeof(unsigned);
-    if (ctx->ready.bytes < ready_bytes) {
-        CKR(ctx->ready.reserve(ready_bytes));
-        CK(cudaMemsetAsync(ctx->ready.p, 0, ctx->ready.bytes, st));
-        ctx->epoch = 0;
-    }
-    CKR(ctx->sync.reserve(256));
-    if (++ctx->epoch >= (1u << 26)) {  // counters carry epoch * 64: restart before they wrap
-        CK(cudaMemsetAsync(ctx->ready.p, 0, ctx->ready.bytes, st));
-        ctx->epoch = 1;
-    }
-    unsigned *next = (unsigned *)ctx->sync.p;
-    int *err = (int *)((char *)ctx->sync.p + 128);
-    CK(cudaMemsetAsync(next, 0, sizeof(unsigned), st));
-    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
-    double prod = 0;
-    for (int s = 0; s < log_m - 1; s++) prod += stage_products(rows, log_m, s, 0) + stage_products(rows, log_m, s + 1, 1);
-    prod += (double)rows * (m / 2) * ADD_P;
-    ctx->prof.begin(FK20_K_FFT_FUSED, prod, st);
-    launch_g1_fused(D, (unsigned *)ctx->ready.p, next, err, ctx->epoch, G, log_m, ctx->sms, st);
-    ctx->prof.end(st);
-    CKL();
-    if (ctx->err_host) CK(cudaMemcpyAsync(ctx->err_host, err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    return 0;
-}
-
-// the inverse + forward transforms of the pipeline, fused or stage by stage
-int run_pipeline_fft(fk20_ctx *ctx, uint4 *D, int G, int rows, int log_m, cudaStream_t st) {
-    if (ctx->err_host && *ctx->err_host) return FK20_ETIMEOUT;  // a previous fused launch gave up
-    if (ctx->fused_fft) return run_hext_to_hfft_fused(ctx, D, G, rows, log_m, st);
-    return run_hext_to_hfft(ctx->prof, D, G, rows, log_m, 0, st);
-}
-
 int output_launch(Profiler &pf, uint64_t *dst, const uint4 *D, const size_t *row_off, int rows, int log_m,
                   int bitrev_out, cudaStream_t st) {
     pf.begin(FK20_K_OUTPUT, (double)rows * (1 << log_m) * 3 * MP, st);
@@ -388,6 +416,12 @@ int build_tables(fk20_ctx *ctx, int log_m, const uint64_t *xext, cudaStream_t st
     const int nbases = L_COLS * m;
     const size_t entries = (size_t)nbases * W * E;
     T->ready = false;
+    T->gen++;
+    if (xext != (const uint64_t *)T->xext.p) {  // keep the bases for rebuilds at another window
+        CKR(T->xext.reserve((size_t)L_COLS * m * sizeof(g1p_t)));
+        CK(cudaMemcpyAsync(T->xext.p, xext, (size_t)L_COLS * m * sizeof(g1p_t), cudaMemcpyDeviceToDevice, st));
+        xext = (const uint64_t *)T->xext.p;
+    }
     T->table.release();
     CKR(T->table.reserve(entries * 6 * sizeof(uint4)));
     // slabs of bases keep the Z scratch near 1 GiB
@@ -410,6 +444,9 @@ int build_tables(fk20_ctx *ctx, int log_m, const uint64_t *xext, cudaStream_t st
     T->log_m = log_m;
     T->cb = cb;
     T->W = W;
+    // complete before returning: later calls may come on other streams (server
+    // slots, plans, non-blocking caller streams) that do not order after `st`
+    CK(cudaStreamSynchronize(st));
     T->ready = true;
     return 0;
 }
@@ -424,38 +461,177 @@ int fingerprint(fk20_ctx *ctx, const void *p, size_t words, unsigned long long *
     return 0;
 }
 
-int msm_launch(Profiler &pf, Tables *T, uint4 *D, const uint4 *S, int G, int rows, int times_m, cudaStream_t st) {
-    MsmArgs a;
-    a.D = D;
-    a.S = S;
-    a.table = (const uint4 *)T->table.p;
-    a.G = G;
-    a.log_m = T->log_m;
-    a.rows = rows;
-    a.cb = T->cb;
-    a.W = T->W;
+int msm_launch(fk20_ctx *ctx, Tables *T, uint4 *D, const uint4 *S, int G, int rows, int times_m, cudaStream_t st) {
+    MsmArgs a{};
+    a.seg[0] = MsmSeg{D, S, (const uint4 *)T->table.p, G, T->log_m, rows, T->cb, T->W, 0};
+    a.nseg = 1;
     a.times_m = times_m;
+    a.warps = (unsigned)G << T->log_m;
     const double prod = (double)rows * L_COLS * (1 << T->log_m) * T->W * MADD_P +
                         (times_m ? (double)rows * (1 << T->log_m) * T->log_m * DBL_P : 0.0);
-    pf.begin(FK20_K_MSM, prod, st);
-    launch_msm(a, st);
-    pf.end(st);
+    ctx->prof.begin(FK20_K_MSM, prod, st);
+    launch_msm(a, ctx->msm_threads, st);
+    ctx->prof.end(st);
     CKL();
     return 0;
 }
 
-// polynomial rows -> tiles of hext_fft (times 1/m unless times_m) in ctx->D
-int pipeline_to_hext(fk20_ctx *ctx, Tables *T, const fr_t *poly, const size_t *row_off, unsigned rows, int times_m,
-                     cudaStream_t st) {
-    const int log_m = T->log_m, m = 1 << log_m;
-    const int G = (int)((rows + 31) / 32);
-    CKR(ctx->S.reserve(scal_bytes(G, m)));
-    CKR(ctx->D.reserve(tile_bytes(G, m)));
-    ctx->prof.begin(FK20_K_TC_FFT, (double)rows * L_COLS * fr_fft_products(log_m), st);
-    launch_tc_fft((uint4 *)ctx->S.p, (const uint64_t *)poly, row_off, (int)T->n, log_m, rows, st);
+// One segment of a pipeline call: `rows` polynomials of length n = 8m
+// (m = 2^log_m); polynomial r starts at word 4 * poly_off[r] of the input and
+// its outputs at word 18 * out_off[r] of the output (device arrays; null =
+// contiguous rows).
+struct Seg {
+    int log_m;
+    unsigned rows;
+    const size_t *poly_off, *out_off;
+};
+
+constexpr size_t SYNC_HDR = 256;  // persistent-launch header: task counter at 0, error flag at 128
+
+struct SegLayout {
+    size_t s_off[MAX_SEGS], d_off[MAX_SEGS], r_off[MAX_SEGS];
+    size_t s_bytes = 0, d_bytes = 0, r_bytes = 0;
+};
+
+int segment_layout(fk20_ctx *ctx, const Seg *sg, int nseg, SegLayout &lay) {
+    if (nseg < 1 || nseg > MAX_SEGS) return FK20_EINVAL;
+    for (int k = 0; k < nseg; k++) {
+        Tables *T = tables_for(ctx, sg[k].log_m);
+        if (!T) return FK20_EINVAL;
+        if (!T->ready) return FK20_ENOSETUP;
+        const int m = 1 << sg[k].log_m, G = (int)((sg[k].rows + 31) / 32);
+        lay.s_off[k] = lay.s_bytes;
+        lay.s_bytes += scal_bytes(G, m);
+        lay.d_off[k] = lay.d_bytes;
+        lay.d_bytes += tile_bytes(G, m);
+        lay.r_off[k] = lay.r_bytes;
+        lay.r_bytes += (size_t)G * m * sizeof(unsigned);
+    }
+    return 0;
+}
+
+// device buffers of a segment call (a no-op once they are large enough)
+int reserve_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, bool full) {
+    SegLayout lay;
+    CKR(segment_layout(ctx, sg, nseg, lay));
+    CKR(ws.init());
+    CKR(ws.S.reserve(lay.s_bytes));
+    CKR(ws.D.reserve(lay.d_bytes));
+    if (full) CKR(ws.sync.reserve(SYNC_HDR + lay.r_bytes));
+    return 0;
+}
+
+// Enqueues the FK20 pipeline of the segments on st: the toeplitz Fr FFTs (one
+// launch per segment), ONE fixed-base MSM launch over all segments, then
+// (full) the G1 inverse + forward transforms as ONE persistent launch over all
+// segments -- or stage by stage when the fused FFT is off -- and the h_fft
+// outputs; or (!full) the hext_fft outputs times m.  The tables are the
+// context's; the workspace is the caller's.  Allocates only when `ws` is too
+// small (reserve_segments first makes the enqueue allocation-free).
+int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr_t *polys, g1p_t *out, bool full,
+                 cudaStream_t st) {
+    SegLayout lay;
+    CKR(segment_layout(ctx, sg, nseg, lay));
+    CKR(reserve_segments(ctx, ws, sg, nseg, full));
+    if (*ws.err_host) return FK20_ETIMEOUT;  // a previous persistent launch gave up: its results are invalid
+    uint4 *S = (uint4 *)ws.S.p, *D = (uint4 *)ws.D.p;
+    const size_t U = sizeof(uint4);
+    for (int k = 0; k < nseg; k++) {
+        Tables *T = tables_for(ctx, sg[k].log_m);
+        ctx->prof.begin(FK20_K_TC_FFT, (double)sg[k].rows * L_COLS * fr_fft_products(sg[k].log_m), st);
+        launch_tc_fft(S + lay.s_off[k] / U, (const uint64_t *)polys, sg[k].poly_off, (int)T->n, sg[k].log_m,
+                      sg[k].rows, st);
+        ctx->prof.end(st);
+        CKL();
+    }
+    MsmArgs a{};
+    double prod = 0;
+    unsigned warps = 0;
+    for (int k = 0; k < nseg; k++) {
+        Tables *T = tables_for(ctx, sg[k].log_m);
+        const int m = 1 << sg[k].log_m, G = (int)((sg[k].rows + 31) / 32);
+        a.seg[k] = MsmSeg{D + lay.d_off[k] / U, S + lay.s_off[k] / U, (const uint4 *)T->table.p, G, sg[k].log_m,
+                          (int)sg[k].rows, T->cb, T->W, warps};
+        warps += (unsigned)G * m;
+        prod += (double)sg[k].rows * L_COLS * m * T->W * MADD_P + (full ? 0.0 : (double)sg[k].rows * m * sg[k].log_m * DBL_P);
+    }
+    a.nseg = nseg;
+    a.times_m = full ? 0 : 1;
+    a.warps = warps;
+    ctx->prof.begin(FK20_K_MSM, prod, st);
+    launch_msm(a, ctx->msm_threads, st);
     ctx->prof.end(st);
     CKL();
-    CKR(msm_launch(ctx->prof, T, (uint4 *)ctx->D.p, (const uint4 *)ctx->S.p, G, (int)rows, times_m, st));
+    if (full && ctx->fused_fft) {
+        FusedPlan p{};
+        unsigned widest = 0;
+        prod = 0;
+        for (int k = 0; k < nseg; k++) {
+            const int log_m = sg[k].log_m, m = 1 << log_m, G = (int)((sg[k].rows + 31) / 32);
+            p.seg[k] = FusedSeg{D + lay.d_off[k] / U, (unsigned *)((char *)ws.sync.p + SYNC_HDR + lay.r_off[k])};
+            p.blk.G[k] = G;
+            p.blk.log_m[k] = log_m;
+            widest += (unsigned)G * (m / 2);
+            for (int s = 0; s < log_m - 1; s++)
+                prod += stage_products((int)sg[k].rows, log_m, s, 0) + stage_products((int)sg[k].rows, log_m, s + 1, 1);
+            prod += (double)sg[k].rows * (m / 2) * ADD_P;
+        }
+        p.blk.nseg = nseg;
+        fused_blocks_build(p.blk);
+        p.next = (unsigned *)ws.sync.p;
+        p.err = (int *)((char *)ws.sync.p + 128);
+        p.epoch = 1;  // counters are cleared before every launch
+        int per_sm = ctx->fused_occupancy;
+        if (ctx->fft_blocks_per_sm > 0 && ctx->fft_blocks_per_sm < per_sm) per_sm = ctx->fft_blocks_per_sm;
+        const unsigned max_blocks = (widest + FFT_WARPS - 1) / FFT_WARPS;
+        p.blocks = (int)std::min<unsigned>((unsigned)(ctx->sms * per_sm), max_blocks);
+        CK(cudaMemsetAsync(ws.sync.p, 0, SYNC_HDR + lay.r_bytes, st));
+        ctx->prof.begin(FK20_K_FFT_FUSED, prod, st);
+        launch_g1_fused(p, st);
+        ctx->prof.end(st);
+        CKL();
+        CK(cudaMemcpyAsync(ws.err_host, p.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    } else if (full) {
+        for (int k = 0; k < nseg; k++)
+            CKR(run_hext_to_hfft(ctx->prof, D + lay.d_off[k] / U, (int)((sg[k].rows + 31) / 32), (int)sg[k].rows,
+                                 sg[k].log_m, 0, st));
+    }
+    for (int k = 0; k < nseg; k++)
+        CKR(output_launch(ctx->prof, (uint64_t *)out, D + lay.d_off[k] / U, sg[k].out_off, (int)sg[k].rows,
+                          sg[k].log_m, 0, st));
+    return 0;
+}
+
+// A ragged batch as segments, one per length (longest first): the offsets go
+// to the workspace's device array through its pinned staging (no host wait
+// unless the previous copy out of the staging is still pending).
+int batch_segments(fk20_ctx *ctx, Workspace &ws, unsigned count, const unsigned *n, const size_t *poly_off,
+                   const size_t *out_off, Seg *sg, int *nseg, cudaStream_t st) {
+    CKR(ws.init());
+    CKR(ws.stage_offsets(2 * (size_t)count));
+    size_t *h = ws.offs_host;
+    size_t at = 0;
+    struct Part { int log_m; size_t first; unsigned rows; } parts[3];
+    int np = 0;
+    for (int log_m = 9; log_m >= 7; log_m--) {
+        const unsigned nn = (unsigned)(L_COLS << (log_m - 1));
+        Part pt{log_m, at, 0};
+        for (unsigned j = 0; j < count; j++)
+            if (n[j] == nn) { h[at++] = poly_off[j]; pt.rows++; }
+        for (unsigned j = 0; j < count; j++)
+            if (n[j] == nn) h[at++] = out_off[j];
+        if (pt.rows) {
+            if (!tables_for(ctx, log_m)->ready) return FK20_ENOSETUP;
+            parts[np++] = pt;
+        }
+    }
+    CKR(ws.offs.reserve(at * sizeof(size_t)));
+    CK(cudaMemcpyAsync(ws.offs.p, h, at * sizeof(size_t), cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(ws.offs_done, st));
+    const size_t *d = (const size_t *)ws.offs.p;
+    for (int k = 0; k < np; k++)
+        sg[k] = Seg{parts[k].log_m, parts[k].rows, d + parts[k].first, d + parts[k].first + parts[k].rows};
+    *nseg = np;
     return 0;
 }
 
@@ -463,6 +639,15 @@ int check_call(const void *out, const void *in, unsigned rows) {
     if (!out || !in) return FK20_EINVAL;
     if (rows == 0 || rows > MAX_ROWS) return FK20_EINVAL;
     if (((uintptr_t)out | (uintptr_t)in) & 15) return FK20_EINVAL;
+    return 0;
+}
+
+int check_batch(const g1p_t *h_fft, const fr_t *polys, unsigned count, const unsigned *n, const size_t *poly_off,
+                const size_t *out_off) {
+    if (!h_fft || !polys || !n || !poly_off || !out_off || count == 0 || count > MAX_ROWS) return FK20_EINVAL;
+    if (((uintptr_t)h_fft | (uintptr_t)polys) & 15) return FK20_EINVAL;
+    for (unsigned j = 0; j < count; j++)
+        if (log_m_for_n(n[j]) < 0) return FK20_EINVAL;
     return 0;
 }
 
@@ -474,7 +659,12 @@ int default_ctx(fk20_ctx **out) {
     int dev;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { cudaGetLastError(); return FK20_ENODEV; }
     std::lock_guard<std::mutex> lk(g_default_mu);
-    if (!g_default[dev]) CKR(fk20_ctx_create(&g_default[dev], dev, 0));
+    if (!g_default[dev]) {
+        // FK20_WINDOW selects the default contexts' table window (8..13); unset = 10
+        int w = 0;
+        if (const char *e = getenv("FK20_WINDOW")) w = atoi(e);
+        CKR(fk20_ctx_create(&g_default[dev], dev, w));
+    }
     *out = g_default[dev];
     return 0;
 }
@@ -562,8 +752,12 @@ int fk20_ctx_create(fk20_ctx **out, int device, int window) {
     if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sms = prop.multiProcessorCount;
     {
         DeviceGuard dg(device);
-        if (cudaMallocHost(&c->err_host, sizeof(int)) == cudaSuccess) *c->err_host = 0;
-        else { cudaGetLastError(); c->err_host = nullptr; }
+        c->fused_occupancy = std::max(1, fused_blocks_per_sm());
+        const int rc = c->ws.init();
+        if (rc) {
+            delete c;
+            return rc;
+        }
     }
     *out = c;
     return 0;
@@ -574,6 +768,14 @@ int fk20_ctx_set(fk20_ctx *ctx, int option, int value) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     switch (option) {
     case FK20_OPT_FUSED_FFT: ctx->fused_fft = value != 0; return 0;
+    case FK20_OPT_MSM_THREADS:
+        if (value != 64 && value != 128 && value != 256) return FK20_EINVAL;
+        ctx->msm_threads = value;
+        return 0;
+    case FK20_OPT_FFT_BLOCKS_PER_SM:
+        if (value < 0 || value > 64) return FK20_EINVAL;
+        ctx->fft_blocks_per_sm = value;
+        return 0;
     default: return FK20_EINVAL;
     }
 }
@@ -583,8 +785,8 @@ int fk20_ctx_status(fk20_ctx *ctx) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     DeviceGuard dg(ctx->device);
     CK(cudaDeviceSynchronize());
-    if (ctx->err_host && *ctx->err_host) {
-        *ctx->err_host = 0;
+    if (ctx->ws.err_host && *ctx->ws.err_host) {
+        *ctx->ws.err_host = 0;
         return FK20_ETIMEOUT;
     }
     return 0;
@@ -595,17 +797,12 @@ int fk20_ctx_destroy(fk20_ctx *ctx) {
     {
         DeviceGuard dg(ctx->device);
         cudaDeviceSynchronize();
-        for (auto &t : ctx->tab) t.table.release();
-        ctx->S.release();
-        ctx->D.release();
+        for (auto &t : ctx->tab) t.table.release(), t.xext.release();
+        ctx->ws.release();
         ctx->D2.release();
         ctx->scratch.release();
         ctx->xext.release();
-        ctx->offs.release();
         ctx->fp_dev.release();
-        ctx->ready.release();
-        ctx->sync.release();
-        if (ctx->err_host) cudaFreeHost(ctx->err_host);
     }
     delete ctx;
     return 0;
@@ -641,8 +838,8 @@ int fk20_program_cost(int index, int *dbl, int *add) {
 
 size_t fk20_ctx_device_bytes(const fk20_ctx *ctx) {
     if (!ctx) return 0;
-    size_t b = ctx->S.bytes + ctx->D.bytes + ctx->D2.bytes + ctx->scratch.bytes + ctx->xext.bytes + ctx->offs.bytes;
-    for (auto &t : ctx->tab) b += t.table.bytes;
+    size_t b = ctx->ws.bytes() + ctx->D2.bytes + ctx->scratch.bytes + ctx->xext.bytes;
+    for (auto &t : ctx->tab) b += t.table.bytes + t.xext.bytes;
     return b;
 }
 
@@ -679,12 +876,8 @@ int fk20_ctx_poly2h_fft(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polynomial, uns
     DeviceGuard dg(ctx->device);
     Tables *T = tables_for(ctx, log_m);
     if (!T->ready) return FK20_ENOSETUP;
-    cudaStream_t st = S_(stream);
-    const int G = (int)((rows + 31) / 32);
-    CKR(pipeline_to_hext(ctx, T, polynomial, nullptr, rows, 0, st));
-    CKR(run_pipeline_fft(ctx, (uint4 *)ctx->D.p, G, (int)rows, log_m, st));
-    CKR(output_launch(ctx->prof, (uint64_t *)h_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st));
-    return 0;
+    const Seg sg{log_m, rows, nullptr, nullptr};
+    return run_segments(ctx, ctx->ws, &sg, 1, polynomial, h_fft, true, S_(stream));
 }
 
 int fk20_ctx_poly2hext_fft(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *polynomial, unsigned rows, unsigned n,
@@ -697,10 +890,8 @@ int fk20_ctx_poly2hext_fft(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *polynomia
     DeviceGuard dg(ctx->device);
     Tables *T = tables_for(ctx, log_m);
     if (!T->ready) return FK20_ENOSETUP;
-    cudaStream_t st = S_(stream);
-    CKR(pipeline_to_hext(ctx, T, polynomial, nullptr, rows, 1, st));
-    CKR(output_launch(ctx->prof, (uint64_t *)hext_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st));
-    return 0;
+    const Seg sg{log_m, rows, nullptr, nullptr};
+    return run_segments(ctx, ctx->ws, &sg, 1, polynomial, hext_fft, false, S_(stream));
 }
 
 int fk20_ctx_msm(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *tc_fft, unsigned rows, unsigned n, void *stream) {
@@ -715,54 +906,269 @@ int fk20_ctx_msm(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *tc_fft, unsigned ro
     cudaStream_t st = S_(stream);
     const int m = 1 << log_m;
     const int G = (int)((rows + 31) / 32);
-    CKR(ctx->S.reserve(scal_bytes(G, m)));
-    CKR(ctx->D.reserve(tile_bytes(G, m)));
-    launch_ref_to_scalars((uint4 *)ctx->S.p, (const uint64_t *)tc_fft, (int)rows, log_m, st);
+    CKR(ctx->ws.S.reserve(scal_bytes(G, m)));
+    CKR(ctx->ws.D.reserve(tile_bytes(G, m)));
+    launch_ref_to_scalars((uint4 *)ctx->ws.S.p, (const uint64_t *)tc_fft, (int)rows, log_m, st);
     CKL();
-    CKR(msm_launch(ctx->prof, T, (uint4 *)ctx->D.p, (const uint4 *)ctx->S.p, G, (int)rows, 1, st));
-    CKR(output_launch(ctx->prof, (uint64_t *)hext_fft, (const uint4 *)ctx->D.p, nullptr, (int)rows, log_m, 0, st));
+    CKR(msm_launch(ctx, T, (uint4 *)ctx->ws.D.p, (const uint4 *)ctx->ws.S.p, G, (int)rows, 1, st));
+    CKR(output_launch(ctx->prof, (uint64_t *)hext_fft, (const uint4 *)ctx->ws.D.p, nullptr, (int)rows, log_m, 0, st));
     return 0;
 }
 
 int fk20_ctx_batch(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polys, unsigned count, const unsigned *n,
                    const size_t *poly_off, const size_t *out_off, void *stream) {
-    if (!ctx || !h_fft || !polys || !n || !poly_off || !out_off || count == 0 || count > MAX_ROWS) return FK20_EINVAL;
-    if (((uintptr_t)h_fft | (uintptr_t)polys) & 15) return FK20_EINVAL;
-    for (unsigned j = 0; j < count; j++)
-        if (log_m_for_n(n[j]) < 0) return FK20_EINVAL;
+    if (!ctx) return FK20_EINVAL;
+    CKR(check_batch(h_fft, polys, count, n, poly_off, out_off));
     std::lock_guard<std::mutex> lk(ctx->mu);
     DeviceGuard dg(ctx->device);
     cudaStream_t st = S_(stream);
-    // group instances by length; one stream-ordered pipeline per length
-    std::vector<size_t> offs;
-    struct Group { int log_m; size_t first; unsigned rows; };
-    std::vector<Group> groups;
-    for (int log_m = 9; log_m >= 7; log_m--) {
-        const unsigned nn = (unsigned)(L_COLS << (log_m - 1));
-        Group gr{log_m, offs.size(), 0};
-        for (unsigned j = 0; j < count; j++)
-            if (n[j] == nn) { offs.push_back(poly_off[j]); gr.rows++; }
-        for (unsigned j = 0; j < count; j++)
-            if (n[j] == nn) offs.push_back(out_off[j]);
-        if (gr.rows) {
-            if (!tables_for(ctx, log_m)->ready) return FK20_ENOSETUP;
-            groups.push_back(gr);
-        }
+    Seg sg[3];
+    int nseg = 0;
+    CKR(batch_segments(ctx, ctx->ws, count, n, poly_off, out_off, sg, &nseg, st));
+    return run_segments(ctx, ctx->ws, sg, nseg, polys, h_fft, true, st);
+}
+
+int fk20_ctx_get(fk20_ctx *ctx, int option, int *value) {
+    if (!ctx || !value) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    switch (option) {
+    case FK20_OPT_FUSED_FFT: *value = ctx->fused_fft; return 0;
+    case FK20_OPT_MSM_THREADS: *value = ctx->msm_threads; return 0;
+    case FK20_OPT_FFT_BLOCKS_PER_SM: *value = ctx->fft_blocks_per_sm; return 0;
+    default: return FK20_EINVAL;
     }
-    CKR(ctx->offs.reserve(offs.size() * sizeof(size_t)));
-    CK(cudaMemcpyAsync(ctx->offs.p, offs.data(), offs.size() * sizeof(size_t), cudaMemcpyHostToDevice, st));
-    const size_t *doffs = (const size_t *)ctx->offs.p;
-    for (const Group &gr : groups) {
-        Tables *T = tables_for(ctx, gr.log_m);
-        const int G = (int)((gr.rows + 31) / 32);
-        CKR(pipeline_to_hext(ctx, T, polys, doffs + gr.first, gr.rows, 0, st));
-        CKR(run_pipeline_fft(ctx, (uint4 *)ctx->D.p, G, (int)gr.rows, gr.log_m, st));
-        CKR(output_launch(ctx->prof, (uint64_t *)h_fft, (const uint4 *)ctx->D.p, doffs + gr.first + gr.rows,
-                          (int)gr.rows, gr.log_m, 0, st));
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batch plans (CUDA graphs)
+struct fk20_plan {
+    fk20_ctx *ctx = nullptr;
+    Workspace ws;
+    cudaStream_t capture = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned gen[3] = {0, 0, 0};
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (capture) cudaStreamDestroy(capture);
+        ws.release();
+        exec = nullptr;
+        graph = nullptr;
+        capture = nullptr;
     }
-    // the host offset array must outlive the copy from pageable memory
-    CK(cudaStreamSynchronize(st));
+};
+
+namespace {
+
+// the batch's launch sequence (offsets already on the device) captured into plan->graph
+int capture_plan(fk20_plan *plan, g1p_t *h_fft, const fr_t *polys, const Seg *sg, int nseg) {
+    fk20_ctx *ctx = plan->ctx;
+    CKR(reserve_segments(ctx, plan->ws, sg, nseg, true));
+    const bool prof_on = ctx->prof.on;
+    ctx->prof.on = false;  // timing events cannot be replayed
+    CK(cudaStreamBeginCapture(plan->capture, cudaStreamCaptureModeThreadLocal));
+    const int rc = run_segments(ctx, plan->ws, sg, nseg, polys, h_fft, true, plan->capture);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(plan->capture, &g);
+    ctx->prof.on = prof_on;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc;
+    }
+    CK(ec);
+    plan->graph = g;
+    CK(cudaGraphInstantiate(&plan->exec, g, 0));
     return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fk20_plan_create(fk20_plan **out, fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polys, unsigned count,
+                     const unsigned *n, const size_t *poly_off, const size_t *out_off) {
+    if (!out || !ctx) return FK20_EINVAL;
+    CKR(check_batch(h_fft, polys, count, n, poly_off, out_off));
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    fk20_plan *plan = new fk20_plan();
+    plan->ctx = ctx;
+    int rc = plan->ws.init();
+    if (!rc && cudaStreamCreateWithFlags(&plan->capture, cudaStreamNonBlocking) != cudaSuccess) rc = (int)cudaGetLastError();
+    Seg sg[3];
+    int nseg = 0;
+    if (!rc) rc = batch_segments(ctx, plan->ws, count, n, poly_off, out_off, sg, &nseg, plan->capture);
+    if (!rc) rc = (int)cudaStreamSynchronize(plan->capture);
+    if (!rc) rc = capture_plan(plan, h_fft, polys, sg, nseg);
+    if (rc) {
+        plan->release();
+        delete plan;
+        return rc;
+    }
+    for (int k = 0; k < 3; k++) plan->gen[k] = ctx->tab[k].gen;
+    *out = plan;
+    return 0;
+}
+
+int fk20_plan_launch(fk20_plan *plan, void *stream) {
+    if (!plan) return FK20_EINVAL;
+    fk20_ctx *ctx = plan->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    for (int k = 0; k < 3; k++)
+        if (plan->gen[k] != ctx->tab[k].gen) return FK20_ENOSETUP;
+    if (*plan->ws.err_host) return FK20_ETIMEOUT;
+    CK(cudaGraphLaunch(plan->exec, S_(stream)));
+    return 0;
+}
+
+int fk20_plan_destroy(fk20_plan *plan) {
+    if (!plan) return FK20_EINVAL;
+    {
+        DeviceGuard dg(plan->ctx->device);
+        cudaDeviceSynchronize();
+        plan->release();
+    }
+    delete plan;
+    return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- autotuner
+namespace {
+
+size_t table_bytes_for(int log_m, int w) {
+    const size_t W = (size_t)(255 + w - 1) / w;
+    return (size_t)L_COLS * ((size_t)1 << log_m) * W * ((size_t)1 << (w - 1)) * 6 * sizeof(uint4);
+}
+
+struct Tuner {
+    fk20_ctx *ctx;
+    int log_m;
+    unsigned rows;
+    cudaStream_t st;
+    const fr_t *poly;
+    g1p_t *out;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    // average ms of one call after one untimed call
+    int time(float *ms) {
+        const Seg sg{log_m, rows, nullptr, nullptr};
+        CKR(run_segments(ctx, ctx->ws, &sg, 1, poly, out, true, st));
+        const int reps = 2;
+        CK(cudaEventRecord(e0, st));
+        for (int r = 0; r < reps; r++) CKR(run_segments(ctx, ctx->ws, &sg, 1, poly, out, true, st));
+        CK(cudaEventRecord(e1, st));
+        CK(cudaEventSynchronize(e1));
+        if (*ctx->ws.err_host) {
+            *ctx->ws.err_host = 0;
+            return FK20_ETIMEOUT;
+        }
+        CK(cudaEventElapsedTime(ms, e0, e1));
+        *ms /= reps;
+        return 0;
+    }
+};
+
+int autotune(fk20_ctx *ctx, int log_m, unsigned rows, size_t max_table_bytes, fk20_tune_result *res, cudaStream_t st) {
+    Tables *T = tables_for(ctx, log_m);
+    if (!T->ready) return FK20_ENOSETUP;
+    const int m = 1 << log_m;
+    const unsigned n = (unsigned)(m * L_COLS / 2);
+    DevBuf poly, out;
+    CKR(poly.reserve((size_t)rows * n * sizeof(fr_t)));
+    CKR(out.reserve((size_t)rows * m * sizeof(g1p_t)));
+    {  // sample coefficients: a SplitMix64 stream masked below 2^253 < r
+        std::vector<uint64_t> h((size_t)rows * n * 4);
+        uint64_t x = 0x5eed5eed5eedull;
+        for (size_t i = 0; i < h.size(); i++) {
+            uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            h[i] = z ^ (z >> 31);
+            if ((i & 3) == 3) h[i] &= (1ull << 61) - 1;
+        }
+        CK(cudaMemcpy(poly.p, h.data(), h.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    }
+    Tuner tu{ctx, log_m, rows, st, (const fr_t *)poly.p, (g1p_t *)out.p};
+    CK(cudaEventCreate(&tu.e0));
+    CK(cudaEventCreate(&tu.e1));
+    struct Cfg { int window, threads, bps, fused; };
+    Cfg best{T->cb, ctx->msm_threads, ctx->fft_blocks_per_sm, ctx->fused_fft};
+    float best_ms = 0;
+    int rc = tu.time(&best_ms);
+    const float ms_default = best_ms;
+    auto apply = [&](const Cfg &c) {
+        ctx->msm_threads = c.threads;
+        ctx->fft_blocks_per_sm = c.bps;
+        ctx->fused_fft = c.fused;
+    };
+    auto consider = [&](const Cfg &c) -> int {
+        apply(c);
+        float ms = 0;
+        CKR(tu.time(&ms));
+        if (ms < best_ms) best_ms = ms, best = c;
+        apply(best);
+        return 0;
+    };
+    // 1. table window, within the memory budget
+    if (!rc) {
+        size_t budget = max_table_bytes;
+        if (!budget) {
+            size_t fr = 0, tot = 0;
+            CK(cudaMemGetInfo(&fr, &tot));
+            const size_t margin = (size_t)4 << 30;
+            budget = fr + T->table.bytes > margin ? fr + T->table.bytes - margin : 0;
+        }
+        const int w0 = T->cb;
+        for (int w = 8; w <= 13 && !rc; w++) {
+            if (w == w0 || table_bytes_for(log_m, w) > budget) continue;
+            ctx->window = w;
+            rc = build_tables(ctx, log_m, (const uint64_t *)T->xext.p, st);
+            float ms = 0;
+            if (!rc) rc = tu.time(&ms);
+            if (!rc && ms < best_ms) best_ms = ms, best.window = w;
+        }
+        if (!rc && T->cb != best.window) {
+            ctx->window = best.window;
+            rc = build_tables(ctx, log_m, (const uint64_t *)T->xext.p, st);
+        }
+        ctx->window = best.window;
+    }
+    // 2. MSM block size, 3. persistent FFT grid, 4. fused vs staged FFT
+    for (int t : {64, 128, 256})
+        if (!rc && t != best.threads) rc = consider(Cfg{best.window, t, best.bps, best.fused});
+    for (int b = 1; b <= ctx->fused_occupancy && !rc; b++)
+        if (b != (best.bps ? best.bps : ctx->fused_occupancy)) rc = consider(Cfg{best.window, best.threads, b, 1});
+    if (!rc) rc = consider(Cfg{best.window, best.threads, best.bps, best.fused ? 0 : 1});
+    apply(best);
+    cudaEventDestroy(tu.e0);
+    cudaEventDestroy(tu.e1);
+    cudaStreamSynchronize(st);
+    if (rc) return rc;
+    res->window = best.window;
+    res->msm_threads = best.threads;
+    res->fft_blocks_per_sm = best.bps;
+    res->fused_fft = best.fused;
+    res->ms = best_ms;
+    res->ms_default = ms_default;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fk20_ctx_autotune(fk20_ctx *ctx, unsigned n, unsigned rows, size_t max_table_bytes, fk20_tune_result *result,
+                      void *stream) {
+    const int log_m = log_m_for_n(n);
+    if (!ctx || !result || log_m < 0 || rows == 0 || rows > 4096) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    return autotune(ctx, log_m, rows, max_table_bytes, result, S_(stream));
 }
 
 // ---------------------------------------------------------------- reference entry points
@@ -951,6 +1357,358 @@ int fk20_bench_field(int field, int sqr, uint32_t *data, size_t count, int iters
     CKR(current_device_ready());
     launch_bench_field(field, sqr, data, count, iters, S_(stream));
     CKL();
+    return 0;
+}
+
+}  // extern "C"
+
+// ============================================================================ request server
+// Continuous batching: one worker thread per server retires finished packs
+// (copies their proofs to the callers' buffers), admits waiting requests into
+// free slots as one mixed-length pack each, and otherwise sleeps until a
+// request arrives or a pack's stream reaches its completion callback.
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Req {
+    uint64_t ticket;
+    const fr_t *poly;
+    unsigned n;
+    g1p_t *out;
+    Clock::time_point t0;
+};
+
+struct Slot {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    Workspace ws;
+    DevBuf dpoly, dout;
+    void *hpoly = nullptr, *hout = nullptr;  // pinned staging of the pack's inputs and outputs
+    size_t hpoly_bytes = 0, hout_bytes = 0;
+    std::vector<Req> reqs;     // the pack in flight (empty: the slot is free)
+    std::vector<size_t> out_at;  // g1p_t offset of each request's proofs in hout
+    int rc = 0;                // error of enqueueing the pack
+    size_t bytes() const { return ws.bytes() + dpoly.bytes + dout.bytes; }
+};
+
+int pinned_reserve(void **p, size_t *have, size_t need) {
+    if (need <= *have) return 0;
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    *have = 0;
+    if (cudaMallocHost(p, need) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return FK20_ENOMEM;
+    }
+    *have = need;
+    return 0;
+}
+
+// device bytes of a pack with cnt[k] requests of log_m = 7 + k
+size_t pack_bytes(const unsigned cnt[3]) {
+    size_t b = SYNC_HDR + 2 * sizeof(size_t) * (cnt[0] + cnt[1] + cnt[2]);
+    for (int k = 0; k < 3; k++) {
+        if (!cnt[k]) continue;
+        const int m = 128 << k, G = (int)((cnt[k] + 31) / 32);
+        b += (size_t)cnt[k] * ((size_t)m * 8 * sizeof(fr_t) + (size_t)m * sizeof(g1p_t));
+        b += scal_bytes(G, m) + tile_bytes(G, m) + (size_t)G * m * sizeof(unsigned);
+    }
+    return b;
+}
+
+}  // namespace
+
+struct fk20_server {
+    fk20_ctx *ctx = nullptr;
+    fk20_server_config cfg{};
+    std::vector<Slot> slots;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Req> queue;
+    std::unordered_set<uint64_t> live;             // submitted and not yet waited for
+    std::unordered_map<uint64_t, int> finished;    // ticket -> status
+    uint64_t next_ticket = 1;
+    bool stop = false, wake = false;
+    std::thread worker;
+    // statistics since the last reset
+    std::vector<double> lat_ms;
+    uint64_t proofs = 0, packs = 0, pack_rows = 0;
+    Clock::time_point first, last;
+    bool started = false;
+};
+
+namespace {
+
+void CUDART_CB pack_done_cb(void *p) {
+    fk20_server *s = (fk20_server *)p;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->wake = true;
+    }
+    s->cv_work.notify_all();
+}
+
+// inputs to pinned staging, one H2D copy, the segment pipeline, one D2H copy
+int enqueue_pack(fk20_server *s, Slot &sl) {
+    const size_t cnt = sl.reqs.size();
+    std::vector<unsigned> ns(cnt);
+    std::vector<size_t> poly_off(cnt), out_off(cnt);
+    size_t in = 0, out = 0;
+    for (size_t i = 0; i < cnt; i++) {
+        ns[i] = sl.reqs[i].n;
+        poly_off[i] = in;
+        out_off[i] = out;
+        in += sl.reqs[i].n;
+        out += sl.reqs[i].n / 8;
+    }
+    sl.out_at = out_off;
+    CKR(pinned_reserve(&sl.hpoly, &sl.hpoly_bytes, in * sizeof(fr_t)));
+    CKR(pinned_reserve(&sl.hout, &sl.hout_bytes, out * sizeof(g1p_t)));
+    CKR(sl.dpoly.reserve(in * sizeof(fr_t)));
+    CKR(sl.dout.reserve(out * sizeof(g1p_t)));
+    for (size_t i = 0; i < cnt; i++)
+        memcpy((fr_t *)sl.hpoly + poly_off[i], sl.reqs[i].poly, (size_t)sl.reqs[i].n * sizeof(fr_t));
+    CK(cudaMemcpyAsync(sl.dpoly.p, sl.hpoly, in * sizeof(fr_t), cudaMemcpyHostToDevice, sl.st));
+    {
+        fk20_ctx *ctx = s->ctx;
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        Seg sg[3];
+        int nseg = 0;
+        CKR(batch_segments(ctx, sl.ws, (unsigned)cnt, ns.data(), poly_off.data(), out_off.data(), sg, &nseg, sl.st));
+        CKR(run_segments(ctx, sl.ws, sg, nseg, (const fr_t *)sl.dpoly.p, (g1p_t *)sl.dout.p, true, sl.st));
+    }
+    CK(cudaMemcpyAsync(sl.hout, sl.dout.p, out * sizeof(g1p_t), cudaMemcpyDeviceToHost, sl.st));
+    CK(cudaLaunchHostFunc(sl.st, pack_done_cb, s));
+    CK(cudaEventRecord(sl.done, sl.st));
+    return 0;
+}
+
+void server_main(fk20_server *s) {
+    cudaSetDevice(s->ctx->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        // 1. retire finished packs
+        bool retired = false;
+        for (Slot &sl : s->slots) {
+            if (sl.reqs.empty()) continue;
+            int status = sl.rc;
+            if (!status) {
+                const cudaError_t q = cudaEventQuery(sl.done);
+                if (q == cudaErrorNotReady) continue;
+                if (q != cudaSuccess) {
+                    cudaGetLastError();
+                    status = (int)q;
+                } else if (*sl.ws.err_host) {
+                    *sl.ws.err_host = 0;  // the next pack of this slot starts clean
+                    status = FK20_ETIMEOUT;
+                }
+            }
+            std::vector<Req> done;
+            done.swap(sl.reqs);
+            lk.unlock();
+            if (!status)
+                for (size_t i = 0; i < done.size(); i++)
+                    memcpy(done[i].out, (const g1p_t *)sl.hout + sl.out_at[i], (size_t)(done[i].n / 8) * sizeof(g1p_t));
+            const Clock::time_point now = Clock::now();
+            lk.lock();
+            for (const Req &r : done) {
+                s->finished[r.ticket] = status;
+                s->lat_ms.push_back(std::chrono::duration<double, std::milli>(now - r.t0).count());
+                s->proofs += r.n / 8;
+            }
+            s->packs++;
+            s->pack_rows += done.size();
+            s->last = now;
+            sl.rc = 0;
+            retired = true;
+        }
+        if (retired) s->cv_done.notify_all();
+        // 2. admit waiting requests into a free slot
+        Slot *fs = nullptr;
+        size_t others = 0;
+        for (Slot &sl : s->slots) {
+            if (!fs && sl.reqs.empty()) fs = &sl;
+            else others += sl.bytes();
+        }
+        if (fs && !s->queue.empty()) {
+            unsigned cnt[3] = {0, 0, 0};
+            while (!s->queue.empty() && fs->reqs.size() < s->cfg.max_rows) {
+                const Req &r = s->queue.front();
+                unsigned c2[3] = {cnt[0], cnt[1], cnt[2]};
+                c2[log_m_for_n(r.n) - 7]++;
+                if (others + std::max(fs->bytes(), pack_bytes(c2)) > s->cfg.hbm_budget) break;
+                cnt[0] = c2[0], cnt[1] = c2[1], cnt[2] = c2[2];
+                fs->reqs.push_back(r);
+                s->queue.pop_front();
+            }
+            if (fs->reqs.empty()) {
+                // not even one request fits next to the packs in flight: wait for them; alone, it never fits
+                bool busy = false;
+                for (Slot &sl : s->slots) busy |= !sl.reqs.empty();
+                if (!busy) {
+                    s->finished[s->queue.front().ticket] = FK20_ENOMEM;
+                    s->queue.pop_front();
+                    s->cv_done.notify_all();
+                    continue;
+                }
+            } else {
+                lk.unlock();
+                fs->rc = enqueue_pack(s, *fs);
+                lk.lock();
+                continue;
+            }
+        }
+        bool busy = false;
+        for (Slot &sl : s->slots) busy |= !sl.reqs.empty();
+        if (s->stop && s->queue.empty() && !busy) break;
+        // 3. sleep until a request arrives or a pack completes (bounded, as a backstop)
+        s->cv_work.wait_for(lk, std::chrono::milliseconds(busy ? 2 : 50), [&] {
+            if (s->wake || s->stop) return true;
+            if (s->queue.empty()) return false;
+            for (Slot &sl : s->slots)
+                if (sl.reqs.empty()) return true;
+            return false;
+        });
+        s->wake = false;
+    }
+}
+
+void server_free(fk20_server *s) {
+    DeviceGuard dg(s->ctx->device);
+    for (Slot &sl : s->slots) {
+        if (sl.st) cudaStreamSynchronize(sl.st);
+        sl.ws.release();
+        sl.dpoly.release();
+        sl.dout.release();
+        if (sl.hpoly) cudaFreeHost(sl.hpoly);
+        if (sl.hout) cudaFreeHost(sl.hout);
+        if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.st) cudaStreamDestroy(sl.st);
+    }
+    s->slots.clear();
+}
+
+}  // namespace
+
+extern "C" {
+
+int fk20_server_create(fk20_server **out, fk20_ctx *ctx, const fk20_server_config *cfg) {
+    if (!out || !ctx) return FK20_EINVAL;
+    fk20_server_config c = cfg ? *cfg : fk20_server_config{};
+    if (!c.max_rows) c.max_rows = 128;
+    if (!c.slots) c.slots = 2;
+    if (!c.max_queue) c.max_queue = 1u << 16;
+    if (c.max_rows > 4096 || c.slots > 8) return FK20_EINVAL;
+    fk20_server *s = new fk20_server();
+    s->ctx = ctx;
+    {
+        DeviceGuard dg(ctx->device);
+        if (!c.hbm_budget) {
+            size_t fr = 0, tot = 0;
+            if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+                cudaGetLastError();
+                delete s;
+                return FK20_ENODEV;
+            }
+            c.hbm_budget = fr / 2;
+        }
+        s->slots.resize(c.slots);
+        int rc = 0;
+        for (Slot &sl : s->slots) {
+            if (!rc && cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) != cudaSuccess) rc = (int)cudaGetLastError();
+            if (!rc && cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) rc = (int)cudaGetLastError();
+            if (!rc) rc = sl.ws.init();
+        }
+        if (rc) {
+            server_free(s);
+            delete s;
+            return rc;
+        }
+    }
+    s->cfg = c;
+    s->worker = std::thread(server_main, s);
+    *out = s;
+    return 0;
+}
+
+int fk20_server_submit(fk20_server *s, const fr_t *poly, unsigned n, g1p_t *h_fft, uint64_t *ticket) {
+    if (!s || !poly || !h_fft || !ticket) return FK20_EINVAL;
+    const int log_m = log_m_for_n(n);
+    if (log_m < 0) return FK20_EINVAL;
+    if (!tables_for(s->ctx, log_m)->ready) return FK20_ENOSETUP;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) return FK20_EINVAL;
+        if (s->queue.size() >= s->cfg.max_queue) return FK20_EAGAIN;
+        const Clock::time_point now = Clock::now();
+        const uint64_t t = s->next_ticket++;
+        s->queue.push_back(Req{t, poly, n, h_fft, now});
+        s->live.insert(t);
+        if (!s->started) s->first = now, s->started = true;
+        *ticket = t;
+    }
+    s->cv_work.notify_all();
+    return 0;
+}
+
+int fk20_server_wait(fk20_server *s, uint64_t ticket, int timeout_ms) {
+    if (!s) return FK20_EINVAL;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (!s->live.count(ticket)) return FK20_EINVAL;
+    auto ready = [&] { return s->finished.count(ticket) != 0; };
+    if (timeout_ms < 0) s->cv_done.wait(lk, ready);
+    else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return FK20_EAGAIN;
+    const int status = s->finished[ticket];
+    s->finished.erase(ticket);
+    s->live.erase(ticket);
+    return status;
+}
+
+int fk20_server_get_stats(fk20_server *s, fk20_server_stats *out) {
+    if (!s || !out) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    fk20_server_stats st{};
+    std::vector<double> v = s->lat_ms;
+    std::sort(v.begin(), v.end());
+    st.requests = v.size();
+    st.proofs = s->proofs;
+    st.packs = s->packs;
+    if (!v.empty()) {
+        st.p50_ms = v[(v.size() - 1) / 2];
+        st.p99_ms = v[std::min(v.size() - 1, (size_t)std::ceil(0.99 * v.size()) - 1)];
+        double sum = 0;
+        for (double x : v) sum += x;
+        st.mean_ms = sum / v.size();
+        st.max_ms = v.back();
+        st.wall_s = std::chrono::duration<double>(s->last - s->first).count();
+        st.proofs_per_s = st.wall_s > 0 ? s->proofs / st.wall_s : 0;
+    }
+    st.mean_pack_rows = s->packs ? (double)s->pack_rows / s->packs : 0;
+    *out = st;
+    return 0;
+}
+
+int fk20_server_reset_stats(fk20_server *s) {
+    if (!s) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->lat_ms.clear();
+    s->proofs = s->packs = s->pack_rows = 0;
+    s->started = false;
+    return 0;
+}
+
+int fk20_server_destroy(fk20_server *s) {
+    if (!s) return FK20_EINVAL;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    server_free(s);
+    delete s;
     return 0;
 }
 

@@ -19,11 +19,12 @@
 #include "launch.h"
 #include "layout.cuh"
 
+#include <algorithm>
+
 namespace fk {
 
 cudaError_t upload_consts_fft() { return upload_module_consts(); }
 
-constexpr int FFT_THREADS = 64;
 // minimum resident blocks per SM requested from ptxas for the stage kernels
 // (caps registers at 65536 / (FFT_THREADS * FK_FFT_MINB))
 #ifndef FK_FFT_MINB
@@ -92,26 +93,20 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__
 
 // ------------------------------------------------------------------ fused stages
 // One persistent launch runs the whole hext -> h_fft sequence of the plain
-// pipeline: inverse DIF stages 0..L-2, the middle stage, forward DIT stages
-// 1..L-1, over G row groups.  Work is a stream of warp tasks (one butterfly
-// of 32 rows) taken in stage-major order from a global counter; a task waits
-// until the two positions it reads were written by the previous stage
-// (per-position counters ready[g][i] = epoch * 64 + stage + 1, published with
-// release semantics after the task's stores).  Every task only waits on tasks
-// handed out before it, which are held by running warps, so the wait always
-// ends; it is still bounded (FUSED_SPIN_LIMIT polls) and on expiry the kernel
-// records an error code and returns instead of hanging.  Tile data written by
-// other SMs is read through L2 (ld.cg) so no stale L1 line is used.
+// pipeline -- inverse DIF stages 0..L-2, the middle stage, forward DIT stages
+// 1..L-1 -- for every segment of the plan (segments may differ in length).
+// Work is a stream of warp tasks (one butterfly of 32 rows) taken in order
+// from a global counter; the stream is cut into blocks of (segment, stage) in
+// stage-major order.  A task waits until the two positions it reads were
+// written by the previous stage of its segment (per-position counters
+// ready[g][i] = epoch * 64 + stage + 1, published with release semantics after
+// the task's stores).  Tasks go only to running warps and a task only waits on
+// tasks of lower index, so the lowest unfinished task never waits and every
+// wait ends, also when not all blocks are resident.  The wait is still bounded
+// (FUSED_SPIN_LIMIT polls): on expiry the kernel records an error code and
+// returns instead of hanging.  Tile data written by other SMs is read through
+// L2 (ld.cg) so no stale L1 line is used.
 constexpr unsigned FUSED_SPIN_LIMIT = 1u << 24;
-
-struct FusedArgs {
-    uint4 *D;
-    unsigned *ready;    // [G][m]
-    unsigned *next;     // task counter (zeroed before the launch)
-    int *err;           // 0 = ok, else 1000 + stage that timed out
-    unsigned epoch;     // distinct per launch, < 2^26
-    int G, log_m;
-};
 
 FK_D void tile_to_slot_cg(const StridedPoint &slot, const uint4 *base, int lane) {
 #pragma unroll
@@ -157,44 +152,27 @@ FK_D bool wait_ready(const unsigned *ra, const unsigned *rb, unsigned need, int 
     return ok != 0;
 }
 
-__global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_fused(FusedArgs a) {
+__global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_fused(const __grid_constant__ FusedPlan P) {
     __shared__ uint32_t slots[36 * PROG_SLOTS][FFT_THREADS];
-    const int m = 1 << a.log_m, L = a.log_m;
     const int lane = threadIdx.x & 31;
-    const int per_stage = a.G * (m >> 1);
-    const int nstages = 2 * L - 1;  // L-1 inverse, middle, L-1 forward
-    const unsigned base = a.epoch * 64u;
+    const unsigned total = P.blk.start[P.blk.nblk];
+    const unsigned base = P.epoch * 64u;
     const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS}, {&slots[36][threadIdx.x], FFT_THREADS},
                                            {&slots[72][threadIdx.x], FFT_THREADS}, {&slots[108][threadIdx.x], FFT_THREADS}};
     for (;;) {
         unsigned task = 0;
-        if (lane == 0) task = atomicAdd(a.next, 1u);
+        if (lane == 0) task = atomicAdd(P.next, 1u);
         task = __shfl_sync(0xffffffffu, task, 0);
-        if (task >= (unsigned)(per_stage * nstages)) return;
-        if (*(volatile int *)a.err) return;
-        const int S = (int)(task / per_stage), t = (int)(task % per_stage);
-        const int g = t % a.G, b = t / a.G;
-        int i0, i1, tix = 0, kind;
-        if (S < L - 1) {  // inverse DIF stage s = S
-            kind = 0;
-            const int half = m >> (S + 1), j = b & (half - 1);
-            i0 = (b / half) * 2 * half + j;
-            i1 = i0 + half;
-            tix = ((m - (j << S)) << (MAX_LOG_M - L)) & 511;
-        } else if (S == L - 1) {  // middle
-            kind = 2;
-            i0 = 2 * b;
-            i1 = 2 * b + 1;
-        } else {  // forward DIT stage s = S - L + 1
-            kind = 1;
-            const int s = S - L + 1, half = 1 << s, j = b & (half - 1);
-            i0 = (b / half) * 2 * half + j;
-            i1 = i0 + half;
-            tix = (j << (L - 1 - s)) << (MAX_LOG_M - L);
-        }
+        if (task >= total) return;
+        if (*(volatile int *)P.err) return;
+        FusedTask t;
+        fused_task_decode(t, P.blk, task);
+        const FusedSeg &a = P.seg[t.seg];
+        const int m = 1 << P.blk.log_m[t.seg];
+        const int S = t.S, g = t.g, i0 = t.i0, i1 = t.i1, tix = t.tix, kind = t.kind;
         unsigned *r0 = a.ready + (size_t)g * m + i0, *r1 = a.ready + (size_t)g * m + i1;
         if (S > 0 && !wait_ready(r0, r1, base + (unsigned)S, lane)) {
-            if (lane == 0) atomicCAS(a.err, 0, 1000 + S);
+            if (lane == 0) atomicCAS(P.err, 0, 1000 + S);
             return;
         }
         uint4 *p0 = a.D + tile_index(g, m, i0);
@@ -249,16 +227,8 @@ int fused_blocks_per_sm() {
     return n;
 }
 
-void launch_g1_fused(uint4 *D, unsigned *ready, unsigned *next, int *err, unsigned epoch, int G, int log_m,
-                     int sms, cudaStream_t st) {
-    FusedArgs a{D, ready, next, err, epoch, G, log_m};
-    int per_sm = fused_blocks_per_sm();
-    if (per_sm < 1) per_sm = 1;
-    const int tasks_warps = G * ((1 << log_m) / 2);
-    int blocks = sms * per_sm;
-    const int max_blocks = (tasks_warps + FFT_THREADS / 32 - 1) / (FFT_THREADS / 32);
-    if (blocks > max_blocks) blocks = max_blocks;
-    k_g1_fused<<<blocks, FFT_THREADS, 0, st>>>(a);
+void launch_g1_fused(const FusedPlan &p, cudaStream_t st) {
+    k_g1_fused<<<p.blocks, FFT_THREADS, 0, st>>>(p);
 }
 
 // last DIF stage + zeroing of the upper half + first DIT stage: pairs

@@ -8,7 +8,6 @@
 // [-2^(cb-1), 2^(cb-1)] and each nonzero digit costs one mixed addition
 // (RCB Algorithm 8) of a gathered 96-byte entry: no doublings at all, against
 // ~255 doublings + ~128 additions per term in the reference's g1p_mul loop.
-// One warp per (column c, group of 32 rows); lanes are rows.
 #if defined(FK_MSM_OUTLINE) && FK_MSM_OUTLINE
 #define FK_FP_MUL_OUTLINE 1
 #endif
@@ -19,17 +18,26 @@
 #ifndef FK_MSM_MINB
 #define FK_MSM_MINB 1
 #endif
+// block sizes the launcher accepts: 64, 128 (default) or 256 threads
+constexpr int MSM_MAX_THREADS = 256;
 
 namespace fk {
 
 cudaError_t upload_consts_msm() { return upload_module_consts(); }
 
-__global__ void __launch_bounds__(128, FK_MSM_MINB) k_msm(MsmArgs a) {
+// One warp per (segment, column c, group g of 32 rows); lanes are rows.
+// Warps are numbered segment by segment, g fastest, so the warps of a block
+// read the same table column.
+__global__ void __launch_bounds__(MSM_MAX_THREADS, FK_MSM_MINB) k_msm(const __grid_constant__ MsmArgs args) {
+    const unsigned warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (warp >= args.warps) return;
+    int k = 0;
+    while (k + 1 < args.nseg && warp >= args.seg[k + 1].warp_start) k++;
+    const MsmSeg &a = args.seg[k];
     const int m = 1 << a.log_m;
-    const int warp = blockIdx.x * 4 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    const int g = warp % a.G, c = warp / a.G;
-    if (c >= m) return;
+    const unsigned wl = warp - a.warp_start;
+    const int g = (int)(wl % (unsigned)a.G), c = (int)(wl / (unsigned)a.G);
     const int row = g * 32 + lane;
     const bool live = row < a.rows;
     const int E = 1 << (a.cb - 1);
@@ -76,14 +84,15 @@ __global__ void __launch_bounds__(128, FK_MSM_MINB) k_msm(MsmArgs a) {
             }
         }
     }
-    if (a.times_m) {
-        for (int k = 0; k < a.log_m; k++) g1_dbl(acc, acc);
+    if (args.times_m) {
+        for (int t = 0; t < a.log_m; t++) g1_dbl(acc, acc);
     }
     tile_store(a.D + tile_index(g, m, c), lane, acc);
 }
 
-void launch_msm(const MsmArgs &a, cudaStream_t st) {
-    k_msm<<<blocks_for((size_t)a.G * (1u << a.log_m), 4), 128, 0, st>>>(a);
+void launch_msm(const MsmArgs &a, int threads, cudaStream_t st) {
+    if (threads != 64 && threads != 128 && threads != 256) threads = 128;
+    k_msm<<<blocks_for(a.warps, (unsigned)threads / 32), threads, 0, st>>>(a);
 }
 
 }  // namespace fk

@@ -4,13 +4,43 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "fused_plan.cuh"
+
 namespace fk {
 
-struct MsmArgs {
+constexpr int FFT_THREADS = 64;  // threads per block of the G1 FFT stage kernels
+constexpr int FFT_WARPS = FFT_THREADS / 32;
+
+// A launch may cover several segments (fused_plan.cuh): runs of FK20
+// instances of one length each; a ragged batch has one per length.
+
+// fixed-base MSM over the segments' scalar tiles S into their point tiles D
+struct MsmSeg {
     uint4 *D;
     const uint4 *S;
     const uint4 *table;
-    int G, log_m, rows, cb, W, times_m;
+    int G, log_m, rows, cb, W;
+    unsigned warp_start;  // first warp (of the launch) that works on this segment
+};
+struct MsmArgs {
+    MsmSeg seg[MAX_SEGS];
+    int nseg, times_m;
+    unsigned warps;  // total warps = sum of G * m
+};
+
+// Persistent stage-fused G1 FFT plan: the segments' tiles and readiness
+// counters, and the task block table (fused_plan.cuh).
+struct FusedSeg {
+    uint4 *D;
+    unsigned *ready;  // [G][m] readiness counters of this segment
+};
+struct FusedPlan {
+    FusedSeg seg[MAX_SEGS];
+    FusedBlocks blk;
+    unsigned *next;  // task counter (zeroed before the launch)
+    int *err;        // 0 = ok, else 1000 + stage that timed out
+    unsigned epoch;  // readiness value base (epoch * 64 + stage + 1), < 2^26
+    int blocks;      // grid size: resident blocks of the persistent launch
 };
 
 // per-module constant upload (one per translation unit)
@@ -28,13 +58,13 @@ void launch_toeplitz_ref(uint64_t *tc, const uint64_t *poly, int n, int log_m, u
 void launch_ref_to_scalars(uint4 *S, const uint64_t *tcf, int rows, int log_m, cudaStream_t st);
 
 // kernels_msm.cu
-void launch_msm(const MsmArgs &a, cudaStream_t st);
+void launch_msm(const MsmArgs &a, int threads, cudaStream_t st);  // threads: 64, 128 or 256
 
 // kernels_fft.cu
 void launch_g1_stage(uint4 *D, int G, int log_m, int s, int kind, cudaStream_t st);
 void launch_g1_middle(uint4 *D, int G, int log_m, int scale, cudaStream_t st);
-void launch_g1_fused(uint4 *D, unsigned *ready, unsigned *next, int *err, unsigned epoch, int G, int log_m,
-                     int sms, cudaStream_t st);
+int fused_blocks_per_sm();
+void launch_g1_fused(const FusedPlan &p, cudaStream_t st);
 void launch_g1_scale(uint4 *D, int G, int log_m, int prog, cudaStream_t st);
 void launch_ref_to_tile(uint4 *D, const uint64_t *src, int rows, int G, int log_m, int bitrev_in, int zero_upper,
                         cudaStream_t st);

@@ -36,14 +36,39 @@ ABI_SYMBOLS = (
     "fr_fft", "fr_ift", "g1p_fft", "g1p_ift", "fr_fft_n", "g1p_fft_n", "fp_op_n", "fr_op_n",
     "g1p_op_n", "fr_eq_n", "g1p_eq_n", "g1a_fromG1p_n", "fk20_bench_field", "fk20_version",
     "fk20_ctx_profile", "fk20_ctx_profile_read", "fk20_program_cost", "fk20_bench_imad",
-    "fk20_ctx_set", "fk20_ctx_status", "g1p_fft_noalloc",
+    "fk20_ctx_set", "fk20_ctx_status", "g1p_fft_noalloc", "fk20_ctx_get", "fk20_plan_create",
+    "fk20_plan_launch", "fk20_plan_destroy", "fk20_ctx_autotune", "fk20_server_create", "fk20_server_submit",
+    "fk20_server_wait", "fk20_server_get_stats", "fk20_server_reset_stats", "fk20_server_destroy",
 )
 
 # kernel kinds of the per-launch profiler (FK20_K_* in the header)
 KINDS = ("tc_fft", "msm", "stage_inv", "stage_fwd", "middle", "output", "fft_fused")
 FK20_ETIMEOUT = 1005
 FK20_ETOOBIG = 1006
+FK20_EAGAIN = 1007
 FK20_OPT_FUSED_FFT = 1
+FK20_OPT_MSM_THREADS = 2
+FK20_OPT_FFT_BLOCKS_PER_SM = 3
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("window", ctypes.c_int), ("msm_threads", ctypes.c_int), ("fft_blocks_per_sm", ctypes.c_int),
+                ("fused_fft", ctypes.c_int), ("ms", ctypes.c_float), ("ms_default", ctypes.c_float)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("max_rows", ctypes.c_uint), ("slots", ctypes.c_uint), ("hbm_budget", ctypes.c_size_t),
+                ("max_queue", ctypes.c_uint)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_uint64), ("proofs", ctypes.c_uint64), ("packs", ctypes.c_uint64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("wall_s", ctypes.c_double), ("proofs_per_s", ctypes.c_double),
+                ("mean_pack_rows", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Fk20Error(RuntimeError):
@@ -110,6 +135,17 @@ def lib() -> ctypes.CDLL:
             "fk20_ctx_set": ([vp, i, i], i),
             "fk20_ctx_status": ([vp], i),
             "g1p_fft_noalloc": ([vp, vp, u, u, i, vp], i),
+            "fk20_ctx_get": ([vp, i, ctypes.POINTER(i)], i),
+            "fk20_plan_create": ([ctypes.POINTER(vp), vp, vp, vp, u, vp, vp, vp], i),
+            "fk20_plan_launch": ([vp, vp], i),
+            "fk20_plan_destroy": ([vp], i),
+            "fk20_ctx_autotune": ([vp, u, u, sz, ctypes.POINTER(TuneResult), vp], i),
+            "fk20_server_create": ([ctypes.POINTER(vp), vp, ctypes.POINTER(ServerConfig)], i),
+            "fk20_server_submit": ([vp, vp, u, vp, ctypes.POINTER(ctypes.c_uint64)], i),
+            "fk20_server_wait": ([vp, ctypes.c_uint64, i], i),
+            "fk20_server_get_stats": ([vp, ctypes.POINTER(ServerStats)], i),
+            "fk20_server_reset_stats": ([vp], i),
+            "fk20_server_destroy": ([vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -202,6 +238,16 @@ class Context:
     def set(self, option: int, value: int):
         call("fk20_ctx_set", self.h, option, value)
 
+    def get(self, option: int) -> int:
+        v = ctypes.c_int()
+        call("fk20_ctx_get", self.h, option, ctypes.byref(v))
+        return v.value
+
+    def autotune(self, n: int, rows: int = 128, max_table_bytes: int = 0) -> dict:
+        r = TuneResult()
+        call("fk20_ctx_autotune", self.h, n, rows, max_table_bytes, ctypes.byref(r), _stream())
+        return {k: getattr(r, k) for k, _ in TuneResult._fields_}
+
     def status(self) -> int:
         return lib().fk20_ctx_status(self.h)
 
@@ -223,3 +269,87 @@ class Context:
 
 def version() -> str:
     return lib().fk20_version().decode()
+
+
+def program_cost(index: int):
+    """(doublings, additions) of fixed-scalar program `index` (w_512^index, or 2^-s at 512 + s)."""
+    d, a = ctypes.c_int(), ctypes.c_int()
+    call("fk20_program_cost", index, ctypes.byref(d), ctypes.byref(a))
+    return d.value, a.value
+
+
+# ------------------------------------------------------------------ batch plans (CUDA graphs)
+class Plan:
+    """A ragged batch layout bound to fixed device buffers, captured into a
+    CUDA graph once; launch() replays it."""
+
+    def __init__(self, ctx: Context, h_fft, polys, ns, poly_off, out_off):
+        cnt = len(ns)
+        h = ctypes.c_void_p()
+        call("fk20_plan_create", ctypes.byref(h), ctx.h, _ptr(h_fft), _ptr(polys), cnt, (ctypes.c_uint * cnt)(*ns),
+             (ctypes.c_size_t * cnt)(*poly_off), (ctypes.c_size_t * cnt)(*out_off))
+        self.h = h
+        self._keep = (ctx, h_fft, polys)
+
+    def launch(self, stream=None):
+        call("fk20_plan_launch", self.h, stream or _stream())
+
+    def close(self):
+        if self.h:
+            call("fk20_plan_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ request server
+class Server:
+    """Continuous-batching request server over a context (fk20_server_*).
+    submit() takes HOST numpy arrays: the polynomial (n x 4 uint64) and the
+    output (n/8 x 18 uint64); both are kept referenced until wait()."""
+
+    def __init__(self, ctx: Context, max_rows: int = 128, slots: int = 2, hbm_budget: int = 0, max_queue: int = 0):
+        cfg = ServerConfig(max_rows, slots, hbm_budget, max_queue)
+        h = ctypes.c_void_p()
+        call("fk20_server_create", ctypes.byref(h), ctx.h, ctypes.byref(cfg))
+        self.h = h
+        self.ctx = ctx
+        self._held = {}
+
+    def submit(self, poly, out) -> int:
+        n = poly.shape[0]
+        t = ctypes.c_uint64()
+        call("fk20_server_submit", self.h, ctypes.c_void_p(poly.ctypes.data), n, ctypes.c_void_p(out.ctypes.data),
+             ctypes.byref(t))
+        self._held[t.value] = (poly, out)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> int:
+        rc = lib().fk20_server_wait(self.h, ticket, timeout_ms)
+        if rc != FK20_EAGAIN:
+            self._held.pop(ticket, None)
+        return rc
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        call("fk20_server_get_stats", self.h, ctypes.byref(st))
+        return st.as_dict()
+
+    def reset_stats(self):
+        call("fk20_server_reset_stats", self.h)
+
+    def close(self):
+        if self.h:
+            call("fk20_server_destroy", self.h)
+            self.h = None
+            self._held.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -46,6 +46,7 @@ typedef struct { fp_t x, y, z; } g1p_t;
 #define FK20_ENODEV 1004   /* no usable sm_100 device */
 #define FK20_ETIMEOUT 1005 /* a persistent launch gave up waiting (results invalid) */
 #define FK20_ETOOBIG 1006  /* request larger than the fixed scratch of a no-allocation entry point */
+#define FK20_EAGAIN 1007   /* server: the request is not finished yet / the queue is full */
 
 /* ------------------------------------------------------------------ context
  * A context owns, on one device, the fixed-base tables built from xext_fft
@@ -59,7 +60,9 @@ typedef struct fk20_ctx fk20_ctx;
 
 /* window: signed-digit width of the fixed-base tables (8..13; 0 = default 10).
  * Table bytes per polynomial length n: 16*m bases * ceil(255/w) windows *
- * 2^(w-1) entries * 96 B (10.5 GB for n = 4096, w = 10). */
+ * 2^(w-1) entries * 96 B (10.5 GB for n = 4096, w = 10).  The default
+ * context behind the reference-signature entry points takes its window from
+ * the environment variable FK20_WINDOW (read once per device), else 10. */
 int fk20_ctx_create(fk20_ctx **ctx, int device, int window);
 int fk20_ctx_destroy(fk20_ctx *ctx);
 
@@ -90,17 +93,53 @@ int fk20_ctx_msm(fk20_ctx *ctx, g1p_t *hext_fft, const fr_t *tc_fft, unsigned ro
 /* Ragged batch: `count` independent FK20 instances, instance j with length
  * n_j in {1024, 2048, 4096}, polynomial at poly_off[j] (in fr_t units from
  * `polys`) and m_j proofs written at out_off[j] (in g1p_t units from `h_fft`).
- * All offset arrays are HOST arrays.  Instances are grouped by length and run
- * as one stream-ordered batch per length. */
+ * All offset arrays are HOST arrays (read before the call returns).  The
+ * instances are grouped into one segment per length, and all segments run in
+ * ONE fixed-base MSM launch and ONE persistent stage-fused G1 FFT launch.
+ * No reference counterpart (the reference proves one length per call). */
 int fk20_ctx_batch(fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polys, unsigned count, const unsigned *n,
                    const size_t *poly_off, const size_t *out_off, void *stream);
+
+/* Batch plan: a fixed ragged batch layout (the arguments of fk20_ctx_batch)
+ * bound to fixed device buffers, captured once into a CUDA graph with its own
+ * workspace; fk20_plan_launch replays the whole batch as one graph launch.
+ * Launches of one plan must be stream-ordered (they share its workspace).  A
+ * plan whose tables were rebuilt since its creation (reload, autotune)
+ * returns FK20_ENOSETUP; fk20_plan_launch returns FK20_ETIMEOUT once a
+ * replay's persistent launch gave up.  No reference counterpart. */
+typedef struct fk20_plan fk20_plan;
+int fk20_plan_create(fk20_plan **plan, fk20_ctx *ctx, g1p_t *h_fft, const fr_t *polys, unsigned count,
+                     const unsigned *n, const size_t *poly_off, const size_t *out_off);
+int fk20_plan_launch(fk20_plan *plan, void *stream);
+int fk20_plan_destroy(fk20_plan *plan);
+
+/* Autotuner (no reference counterpart): times the pipeline for length n on
+ * `rows` seeded sample rows under each candidate -- table window 8..13 whose
+ * tables fit in max_table_bytes (0 = what the free device memory allows),
+ * MSM block size 64/128/256, persistent FFT grid 1..max blocks per SM, fused
+ * or staged FFT -- one parameter at a time, keeps the fastest in the context
+ * (tables rebuilt at the chosen window) and reports it.  Needs the tables of
+ * n loaded.  Synchronous; takes seconds (one table build per window). */
+typedef struct {
+    int window, msm_threads, fft_blocks_per_sm, fused_fft;
+    float ms;          /* best time for `rows` rows */
+    float ms_default;  /* time of the configuration the context had before */
+} fk20_tune_result;
+int fk20_ctx_autotune(fk20_ctx *ctx, unsigned n, unsigned rows, size_t max_table_bytes, fk20_tune_result *result,
+                      void *stream);
 
 /* Options.  FK20_OPT_FUSED_FFT (default 1): run the inverse and forward G1
  * FFT stages of the pipeline as one persistent launch whose warps take
  * butterfly tasks in stage order and wait (bounded) for their inputs, instead
  * of one launch per stage. */
 #define FK20_OPT_FUSED_FFT 1
+/* FK20_OPT_MSM_THREADS: MSM block size, 64, 128 (default) or 256 threads. */
+#define FK20_OPT_MSM_THREADS 2
+/* FK20_OPT_FFT_BLOCKS_PER_SM: persistent FFT grid, blocks per SM (0 =
+ * default: as many as fit). */
+#define FK20_OPT_FFT_BLOCKS_PER_SM 3
 int fk20_ctx_set(fk20_ctx *ctx, int option, int value);
+int fk20_ctx_get(fk20_ctx *ctx, int option, int *value);
 
 /* Waits for the context's queued work; returns FK20_ETIMEOUT if a persistent
  * launch gave up waiting (its outputs are then invalid), else 0 or a CUDA
@@ -131,6 +170,46 @@ int fk20_ctx_profile_read(fk20_ctx *ctx, int kind, double *ms, long *launches, d
 /* Doublings and additions of the fixed-scalar G1 program `index` (0..511:
  * w_512^index; 512 + s: 2^-s), for work accounting. */
 int fk20_program_cost(int index, int *dbl, int *add);
+
+/* ------------------------------------------------------------------ request server
+ * Continuous batching of blob-proof requests (no reference counterpart: the
+ * reference has no serving layer).  A worker thread admits requests as they
+ * arrive: whenever one of `slots` slots (a stream, a workspace, device and
+ * pinned staging buffers) is free, it packs the waiting requests -- mixed
+ * lengths, first come first served -- up to max_rows and the device-memory
+ * budget, and enqueues them as one segment pipeline (one MSM launch and one
+ * persistent G1 FFT launch over all lengths).  Packs of different slots
+ * overlap on the device; requests that arrive meanwhile wait for the next
+ * free slot.  The setup tables stay resident in the context (load every
+ * length the requests use first).  Each request's result is the same as a
+ * fk20_ctx_poly2h_fft of that polynomial alone.
+ */
+typedef struct fk20_server fk20_server;
+typedef struct {
+    unsigned max_rows;  /* requests per pack (1..4096; 0 = 128) */
+    unsigned slots;     /* packs in flight at once (1..8; 0 = 2) */
+    size_t hbm_budget;  /* device bytes all slots' buffers may hold (0 = half the free memory at creation) */
+    unsigned max_queue; /* waiting requests beyond which submit returns FK20_EAGAIN (0 = 1 << 16) */
+} fk20_server_config;
+typedef struct {
+    uint64_t requests, proofs, packs;
+    double p50_ms, p99_ms, mean_ms, max_ms; /* latency: submit -> proofs in the caller's buffer */
+    double wall_s;                          /* first submit -> last completion since the last reset */
+    double proofs_per_s;                    /* proofs / wall_s */
+    double mean_pack_rows;
+} fk20_server_stats;
+int fk20_server_create(fk20_server **srv, fk20_ctx *ctx, const fk20_server_config *cfg);
+/* poly: HOST array of n fr_t (n in 1024, 2048, 4096); h_fft: HOST array of
+ * 2n/16 g1p_t.  Both must stay valid until fk20_server_wait reports the
+ * ticket done. */
+int fk20_server_submit(fk20_server *srv, const fr_t *poly, unsigned n, g1p_t *h_fft, uint64_t *ticket);
+/* 0: done, result written (the ticket is then forgotten); FK20_EAGAIN: not
+ * done within timeout_ms (< 0 waits without limit); else the error of its pack. */
+int fk20_server_wait(fk20_server *srv, uint64_t ticket, int timeout_ms);
+int fk20_server_get_stats(fk20_server *srv, fk20_server_stats *stats);
+int fk20_server_reset_stats(fk20_server *srv);
+/* Finishes every submitted request, then stops the worker and frees the slots. */
+int fk20_server_destroy(fk20_server *srv);
 
 /* ------------------------------------------------------------------ reference entry points
  * These use a process-wide default context on the current device; tables are

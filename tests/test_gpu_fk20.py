@@ -235,3 +235,129 @@ def test_fused_and_staged_fft_agree(engine):
     assert ctx.status() == 0
     import torch
     assert torch.equal(a, b)
+
+
+def _eq_count(engine, a, b):
+    import torch
+    cnt = a.numel() // 18
+    eq = torch.zeros(cnt, dtype=torch.uint8, device="cuda")
+    engine.call("g1p_eq_n", ctypes.c_void_p(eq.data_ptr()), engine._ptr(a), engine._ptr(b), cnt, engine._stream())
+    return int(eq.sum()), cnt
+
+
+def ragged_instances(count, seed):
+    """count instances with lengths drawn uniformly from {1024, 2048, 4096}."""
+    rng = np.random.default_rng(seed)
+    sizes = [int(x) for x in rng.choice([1024, 2048, 4096], count)]
+    poly_off, out_off, po, oo = [], [], 0, 0
+    for n in sizes:
+        poly_off.append(po)
+        out_off.append(oo)
+        po += n
+        oo += n // 8
+    return sizes, poly_off, out_off, po, oo
+
+
+def test_ragged_1000_instances_one_launch_each(engine):
+    """1000 instances of lengths drawn from {1024, 2048, 4096} in one call (one
+    MSM launch + one persistent G1 FFT launch over three segments) equal the
+    plain per-length path, proof by proof."""
+    import torch
+    sizes, poly_off, out_off, po, oo = ragged_instances(1000, 2024)
+    polys = O.seeded_fr(606, po)
+    c = engine.Context(0)
+    for n in (1024, 2048, 4096):
+        c.load_xext_fft(n, engine.to_device(fk20_setup_data(n)[2]))
+    dpolys = engine.to_device(polys)
+    out = engine.empty((oo, 18))
+    c.profile(True)
+    c.batch(out, dpolys, sizes, poly_off, out_off)
+    prof = c.profile_read()
+    c.profile(False)
+    assert prof["msm"][1] == 1 and prof["fft_fused"][1] == 1
+    assert c.status() == 0
+    # per-length reference: the rows of each length as one contiguous plain call
+    exp = engine.empty((oo, 18))
+    for n in (1024, 2048, 4096):
+        idx = [j for j, s in enumerate(sizes) if s == n]
+        rows = torch.stack([dpolys[poly_off[j]:poly_off[j] + n] for j in idx])
+        h = engine.empty((len(idx), n // 8, 18))
+        c.poly2h_fft(h, rows, len(idx), n)
+        for r, j in enumerate(idx):
+            exp[out_off[j]:out_off[j] + n // 8] = h[r]
+    torch.cuda.synchronize()
+    assert torch.equal(out, exp)
+    # spot-check against the oracle
+    for j in (0, 999):
+        n = sizes[j]
+        ref = O.fk20_row(polys[poly_off[j]:poly_off[j] + n], fk20_setup_data(n)[2])["h_fft"]
+        assert np.array_equal(norm(engine.to_host(out[out_off[j]:out_off[j] + n // 8])), ref)
+    c.close()
+
+
+def test_batch_plan_graph_replay(engine):
+    """A ragged batch captured once into a CUDA graph (fk20_plan_*) gives the
+    same proofs as the direct call, replay after replay, and refuses to replay
+    once its tables were rebuilt."""
+    import torch
+    sizes, poly_off, out_off, po, oo = ragged_instances(70, 99)
+    polys = engine.to_device(O.seeded_fr(707, po))
+    c = engine.Context(0, 8)
+    for n in (1024, 2048, 4096):
+        c.load_xext_fft(n, engine.to_device(fk20_setup_data(n)[2]))
+    exp = engine.empty((oo, 18))
+    c.batch(exp, polys, sizes, poly_off, out_off)
+    out = engine.empty((oo, 18))
+    plan = engine.Plan(c, out, polys, sizes, poly_off, out_off)
+    for _ in range(3):
+        out.zero_()
+        plan.launch()
+        torch.cuda.synchronize()
+        assert torch.equal(out, exp)
+    c.load_xext_fft(2048, engine.to_device(fk20_setup_data(2048)[2]))
+    with pytest.raises(engine.Fk20Error) as e:
+        plan.launch()
+    assert e.value.code == engine.FK20_ENOSETUP
+    plan.close()
+    c.close()
+
+
+def test_launch_shape_options_agree(engine):
+    """MSM block sizes and persistent-grid widths change scheduling only."""
+    import torch
+    n, rows, m = 2048, 45, 256
+    ctx = ctx_for(engine, n)
+    poly = engine.to_device(O.seeded_fr(808, rows * n).reshape(rows, n, 4))
+    ref = engine.empty((rows, m, 18))
+    ctx.poly2h_fft(ref, poly, rows, n)
+    for opt, val in ((engine.FK20_OPT_MSM_THREADS, 64), (engine.FK20_OPT_MSM_THREADS, 256),
+                     (engine.FK20_OPT_FFT_BLOCKS_PER_SM, 1)):
+        old = ctx.get(opt)
+        ctx.set(opt, val)
+        h = engine.empty((rows, m, 18))
+        ctx.poly2h_fft(h, poly, rows, n)
+        ctx.set(opt, old)
+        torch.cuda.synchronize()
+        assert torch.equal(h, ref), (opt, val)
+    with pytest.raises(engine.Fk20Error):
+        ctx.set(engine.FK20_OPT_MSM_THREADS, 96)
+
+
+def test_autotune_keeps_results(engine):
+    """The autotuner picks a window within the table budget and launch shapes;
+    the tuned context still gives the same proofs."""
+    n, rows, m = 1024, 40, 128
+    c = engine.Context(0, 9)
+    c.load_xext_fft(n, engine.to_device(fk20_setup_data(n)[2]))
+    poly = engine.to_device(O.seeded_fr(909, rows * n).reshape(rows, n, 4))
+    before = engine.empty((rows, m, 18))
+    c.poly2h_fft(before, poly, rows, n)
+    res = c.autotune(n, rows=64, max_table_bytes=3 << 30)
+    assert 8 <= res["window"] <= 10 and res["msm_threads"] in (64, 128, 256)
+    assert res["ms"] <= res["ms_default"] * 1.05
+    assert c.get(engine.FK20_OPT_MSM_THREADS) == res["msm_threads"]
+    after = engine.empty((rows, m, 18))
+    c.poly2h_fft(after, poly, rows, n)
+    assert _eq_count(engine, before, after) == (rows * m, rows * m)
+    assert c.status() == 0
+    c.close()

@@ -1,0 +1,76 @@
+"""The continuous-batching request server (fk20_server_*): requests of mixed
+lengths submitted while others are on the GPU are packed and overlapped, and
+every result is bit-identical to proving that polynomial alone."""
+import time
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import fk20_setup_data
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def served_ctx(engine):
+    c = engine.Context(0, 8)
+    for n in (1024, 2048, 4096):
+        c.load_xext_fft(n, engine.to_device(fk20_setup_data(n)[2]))
+    yield c
+    c.close()
+
+
+def test_server_results_same_alone_and_in_the_mix(engine, served_ctx):
+    import torch
+    rng = np.random.default_rng(5)
+    sizes = [int(x) for x in rng.choice([1024, 2048, 4096], 90, p=[0.2, 0.3, 0.5])]
+    polys = [O.seeded_fr(4000 + j, n) for j, n in enumerate(sizes)]
+    outs = [np.zeros((n // 8, 18), np.uint64) for n in sizes]
+    srv = engine.Server(served_ctx, max_rows=16, slots=2)
+    tickets = []
+    for j, n in enumerate(sizes):  # arrivals spread over time, so packs overlap with new arrivals
+        tickets.append(srv.submit(polys[j], outs[j]))
+        if j % 10 == 9:
+            time.sleep(0.002)
+    for t in tickets:
+        assert srv.wait(t, 60000) == 0
+    st = srv.stats()
+    assert st["requests"] == len(sizes) and st["proofs"] == sum(n // 8 for n in sizes)
+    assert st["packs"] >= len(sizes) // 16 and 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
+    srv.close()
+    # each result equals that polynomial proved alone
+    for j, n in enumerate(sizes):
+        h = engine.empty((1, n // 8, 18))
+        served_ctx.poly2h_fft(h, engine.to_device(polys[j].reshape(1, n, 4)), 1, n)
+        assert np.array_equal(engine.to_host(h)[0], outs[j]), j
+    # and the proofs are the oracle's
+    for j in (0, len(sizes) - 1):
+        exp = O.fk20_row(polys[j], fk20_setup_data(sizes[j])[2])["h_fft"]
+        assert np.array_equal(O.g1_normalize(outs[j]), exp)
+
+
+def test_server_rejects_bad_requests(engine, served_ctx):
+    srv = engine.Server(served_ctx, max_rows=8, slots=1)
+    bad = np.zeros((3000, 4), np.uint64)
+    with pytest.raises(engine.Fk20Error) as e:
+        srv.submit(bad, np.zeros((375, 18), np.uint64))
+    assert e.value.code == engine.FK20_EINVAL
+    assert srv.wait(12345, 0) == engine.FK20_EINVAL
+    p = O.seeded_fr(1, 1024)
+    o = np.zeros((128, 18), np.uint64)
+    t = srv.submit(p, o)
+    assert srv.wait(t, 60000) == 0
+    assert srv.wait(t, 0) == engine.FK20_EINVAL  # already collected
+    srv.close()
+
+
+def test_server_without_tables_for_a_length(engine):
+    c = engine.Context(0, 8)
+    c.load_xext_fft(1024, engine.to_device(fk20_setup_data(1024)[2]))
+    srv = engine.Server(c, max_rows=4, slots=1)
+    with pytest.raises(engine.Fk20Error) as e:
+        srv.submit(O.seeded_fr(2, 4096), np.zeros((512, 18), np.uint64))
+    assert e.value.code == engine.FK20_ENOSETUP
+    srv.close()
+    c.close()

@@ -100,3 +100,64 @@ def test_glv_programs_match_scalar_multiplication(emul):
         exp = O.g1_op("mul", pts, np.tile(O.int_to_limbs(k, 4), (len(pts), 1)))
         assert np.array_equal(O.g1_normalize(out), exp), hex(k)
         assert d.value <= 129 and a.value <= 100
+
+
+def fused_schedule(emul, G, log_m):
+    nseg = len(G)
+    cap = sum(g * (1 << l) // 2 * (2 * l - 1) for g, l in zip(G, log_m))
+    out = np.zeros((cap, 7), np.int32)
+    ga, la = (ctypes.c_int * nseg)(*G), (ctypes.c_int * nseg)(*log_m)
+    n = emul.emul_fused_schedule(nseg, ga, la, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.c_long(cap))
+    assert n == cap
+    return out
+
+
+@pytest.mark.parametrize("G,log_m", [([1], [9]), ([3, 2, 5], [9, 8, 7]), ([1, 1, 1, 2], [7, 9, 7, 8])])
+def test_fused_fft_schedule(emul, G, log_m):
+    """The persistent launch's task order (csrc/fused_plan.cuh, decoded the way
+    the kernel decodes it): every stage of every segment touches each position
+    of each row group exactly once, every task only depends on tasks of lower
+    index (so the bounded waits always end), and running the butterflies in
+    task order on Fr values gives FFT(upper half zeroed(IFFT without 1/m)) per
+    segment -- the hext_fft -> h_fft map of the pipeline."""
+    emul.emul_fused_schedule.restype = ctypes.c_long
+    sched = fused_schedule(emul, G, log_m)
+    R = O.R
+    w512 = O.root_of_unity(512)
+    rng = np.random.default_rng(7)
+    vals = {}
+    for k, (g_cnt, L) in enumerate(zip(G, log_m)):
+        for g in range(g_cnt):
+            vals[(k, g)] = [int(x) % R for x in rng.integers(0, 2**62, 1 << L)]
+    start = {key: list(v) for key, v in vals.items()}
+    last_writer = {}  # (seg, g, pos) -> (stage, task index)
+    seen = set()
+    for t, (seg, S, g, i0, i1, tix, kind) in enumerate(sched.tolist()):
+        for p in (i0, i1):
+            key = (seg, S, g, p)
+            assert key not in seen
+            seen.add(key)
+            if S > 0:
+                st, idx = last_writer[(seg, g, p)]
+                assert st == S - 1 and idx < t
+            last_writer[(seg, g, p)] = (S, t)
+        v = vals[(seg, g)]
+        wt = pow(w512, tix, R)
+        u, x = v[i0], v[i1]
+        if kind == 0:
+            v[i0], v[i1] = (u + x) % R, (u - x) * wt % R
+        elif kind == 2:
+            v[i0] = v[i1] = (u + x) % R
+        else:
+            x = x * wt % R
+            v[i0], v[i1] = (u + x) % R, (u - x) % R
+    for k, (g_cnt, L) in enumerate(zip(G, log_m)):
+        m = 1 << L
+        assert len([s for s in seen if s[0] == k]) == g_cnt * m * (2 * L - 1)
+        wp = [pow(w512, (512 // m) * e, R) for e in range(m)]  # powers of w_m
+        for g in range(g_cnt):
+            x = start[(k, g)]
+            inv = [sum(x[j] * wp[(-i * j) % m] for j in range(m)) % R for i in range(m)]
+            inv[m // 2:] = [0] * (m // 2)
+            fwd = [sum(inv[j] * wp[(i * j) % m] for j in range(m)) % R for i in range(m)]
+            assert vals[(k, g)] == fwd, (k, g)
