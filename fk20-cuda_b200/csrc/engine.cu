@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -1430,7 +1431,8 @@ struct fk20_server {
     std::unordered_set<uint64_t> live;             // submitted and not yet waited for
     std::unordered_map<uint64_t, int> finished;    // ticket -> status
     uint64_t next_ticket = 1;
-    bool stop = false, wake = false;
+    bool stop = false;
+    std::atomic<bool> wake{false};  // set by the completion callback, which never takes `mu`
     std::thread worker;
     // statistics since the last reset
     std::vector<double> lat_ms;
@@ -1441,12 +1443,13 @@ struct fk20_server {
 
 namespace {
 
+// Runs on CUDA's callback thread between a pack's last copy and its event:
+// it must not block (the event, and so the slot, would never complete), so it
+// only sets a flag and notifies; the worker's waits are bounded in case the
+// notification lands before the worker sleeps.
 void CUDART_CB pack_done_cb(void *p) {
     fk20_server *s = (fk20_server *)p;
-    {
-        std::lock_guard<std::mutex> g(s->mu);
-        s->wake = true;
-    }
+    s->wake.store(true);
     s->cv_work.notify_all();
 }
 
@@ -1533,26 +1536,54 @@ void server_main(fk20_server *s) {
             else others += sl.bytes();
         }
         if (fs && !s->queue.empty()) {
+            // Oldest first, up to max_rows and the memory budget.  When more
+            // requests wait than a pack takes, each length with 32 or more in
+            // the pack keeps a multiple of 32 (a warp proves 32 rows of one
+            // length; a partial group idles lanes): its youngest extra
+            // requests go back to the head of the queue for the next pack.
+            const bool more = s->queue.size() > s->cfg.max_rows;
             unsigned cnt[3] = {0, 0, 0};
-            while (!s->queue.empty() && fs->reqs.size() < s->cfg.max_rows) {
-                const Req &r = s->queue.front();
+            size_t q = 0;
+            for (; q < s->queue.size() && fs->reqs.size() < s->cfg.max_rows; q++) {
+                const Req &r = s->queue[q];
+                const int k = log_m_for_n(r.n) - 7;
                 unsigned c2[3] = {cnt[0], cnt[1], cnt[2]};
-                c2[log_m_for_n(r.n) - 7]++;
+                c2[k]++;
                 if (others + std::max(fs->bytes(), pack_bytes(c2)) > s->cfg.hbm_budget) break;
-                cnt[0] = c2[0], cnt[1] = c2[1], cnt[2] = c2[2];
+                cnt[k]++;
                 fs->reqs.push_back(r);
-                s->queue.pop_front();
+            }
+            s->queue.erase(s->queue.begin(), s->queue.begin() + (long)q);
+            if (more) {
+                unsigned keep[3];
+                for (int k = 0; k < 3; k++) keep[k] = cnt[k] >= 32 ? cnt[k] & ~31u : cnt[k];
+                std::vector<Req> kept, back;
+                for (size_t t = fs->reqs.size(); t-- > 0;) {
+                    const int k = log_m_for_n(fs->reqs[t].n) - 7;
+                    if (cnt[k] > keep[k]) {
+                        back.push_back(fs->reqs[t]);
+                        cnt[k]--;
+                    } else {
+                        kept.push_back(fs->reqs[t]);
+                    }
+                }
+                fs->reqs.assign(kept.rbegin(), kept.rend());
+                s->queue.insert(s->queue.begin(), back.rbegin(), back.rend());
             }
             if (fs->reqs.empty()) {
-                // not even one request fits next to the packs in flight: wait for them; alone, it never fits
+                // not even one request fits next to the packs in flight: wait
+                // for one of them to complete; alone, it never fits
                 bool busy = false;
                 for (Slot &sl : s->slots) busy |= !sl.reqs.empty();
                 if (!busy) {
                     s->finished[s->queue.front().ticket] = FK20_ENOMEM;
                     s->queue.pop_front();
                     s->cv_done.notify_all();
-                    continue;
+                } else {
+                    s->cv_work.wait_for(lk, std::chrono::milliseconds(2), [&] { return s->wake.load() || s->stop; });
+                    s->wake.store(false);
                 }
+                continue;
             } else {
                 lk.unlock();
                 fs->rc = enqueue_pack(s, *fs);
@@ -1565,13 +1596,13 @@ void server_main(fk20_server *s) {
         if (s->stop && s->queue.empty() && !busy) break;
         // 3. sleep until a request arrives or a pack completes (bounded, as a backstop)
         s->cv_work.wait_for(lk, std::chrono::milliseconds(busy ? 2 : 50), [&] {
-            if (s->wake || s->stop) return true;
+            if (s->wake.load() || s->stop) return true;
             if (s->queue.empty()) return false;
             for (Slot &sl : s->slots)
                 if (sl.reqs.empty()) return true;
             return false;
         });
-        s->wake = false;
+        s->wake.store(false);
     }
 }
 
@@ -1597,7 +1628,7 @@ extern "C" {
 int fk20_server_create(fk20_server **out, fk20_ctx *ctx, const fk20_server_config *cfg) {
     if (!out || !ctx) return FK20_EINVAL;
     fk20_server_config c = cfg ? *cfg : fk20_server_config{};
-    if (!c.max_rows) c.max_rows = 128;
+    if (!c.max_rows) c.max_rows = 512;
     if (!c.slots) c.slots = 2;
     if (!c.max_queue) c.max_queue = 1u << 16;
     if (c.max_rows > 4096 || c.slots > 8) return FK20_EINVAL;

@@ -176,8 +176,9 @@ int fk20_program_cost(int index, int *dbl, int *add);
  * reference has no serving layer).  A worker thread admits requests as they
  * arrive: whenever one of `slots` slots (a stream, a workspace, device and
  * pinned staging buffers) is free, it packs the waiting requests -- mixed
- * lengths, first come first served -- up to max_rows and the device-memory
- * budget, and enqueues them as one segment pipeline (one MSM launch and one
+ * lengths, oldest first, whole groups of 32 rows per length when more are
+ * waiting than a pack takes -- up to max_rows and the device-memory budget,
+ * and enqueues them as one segment pipeline (one MSM launch and one
  * persistent G1 FFT launch over all lengths).  Packs of different slots
  * overlap on the device; requests that arrive meanwhile wait for the next
  * free slot.  The setup tables stay resident in the context (load every
@@ -186,7 +187,7 @@ int fk20_program_cost(int index, int *dbl, int *add);
  */
 typedef struct fk20_server fk20_server;
 typedef struct {
-    unsigned max_rows;  /* requests per pack (1..4096; 0 = 128) */
+    unsigned max_rows;  /* requests per pack (1..4096; 0 = 512) */
     unsigned slots;     /* packs in flight at once (1..8; 0 = 2) */
     size_t hbm_budget;  /* device bytes all slots' buffers may hold (0 = half the free memory at creation) */
     unsigned max_queue; /* waiting requests beyond which submit returns FK20_EAGAIN (0 = 1 << 16) */
