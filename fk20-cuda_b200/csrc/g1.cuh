@@ -205,6 +205,19 @@ FK_HD void g1_dbl(G1P &R, const G1P &P) {
     R.z = Z3;
 }
 
+// affine normalisation in Montgomery form: (x, y, 1) or infinity (0, 1, 0)
+FK_HD void g1_normalize(G1P &p) {
+    if (f_is_zero(p.z)) {
+        g1_set_inf(p);
+        return;
+    }
+    Fp zi;
+    f_inv(zi, p.z);
+    f_mul(p.x, p.x, zi);
+    f_mul(p.y, p.y, zi);
+    f_set_one(p.z);
+}
+
 // GLV endomorphism phi(x, y) = (beta x, y) = [lambda] P on G1, with
 // lambda = z^2 - 1 (z = -0xd201000000010000) and beta the cube root of unity
 // in Fp below (Montgomery form).  r = lambda^2 + lambda + 1.

@@ -48,16 +48,6 @@ __global__ void k_field_op(int op, uint64_t *out, const uint64_t *a, const uint6
     }
 }
 
-// affine normalisation in Montgomery form: (x, y, 1) or infinity (0, 1, 0)
-__device__ void g1_normalize(G1P &p) {
-    if (f_is_zero(p.z)) { g1_set_inf(p); return; }
-    Fp zi;
-    f_inv(zi, p.z);
-    f_mul(p.x, p.x, zi);
-    f_mul(p.y, p.y, zi);
-    f_set_one(p.z);
-}
-
 // Y^2 Z == X^3 + 4 Z^3, or infinity (0, Y != 0, 0)   (g1p_ispoint.cu:14-60)
 __device__ bool g1_on_curve(const G1P &p) {
     if (f_is_zero(p.z)) return !f_is_zero(p.y) && f_is_zero(p.x);

@@ -59,6 +59,10 @@ void launch_ref_to_scalars(uint4 *S, const uint64_t *tcf, int rows, int log_m, c
 
 // kernels_msm.cu
 void launch_msm(const MsmArgs &a, int threads, cudaStream_t st);  // threads: 64, 128 or 256
+// KZG commitments: bases per pass-1 warp; part holds (rows/32) x (n/COMMIT_CHUNK) point tiles
+constexpr int COMMIT_CHUNK = 32;
+void launch_commit(uint64_t *out, uint4 *part, const uint64_t *poly, const uint4 *table, int rows, int n, int W,
+                   int cb, cudaStream_t st);
 
 // kernels_fft.cu
 void launch_g1_stage(uint4 *D, int G, int log_m, int s, int kind, cudaStream_t st);
@@ -72,6 +76,12 @@ void launch_tile_to_ref(uint64_t *dst, const uint4 *D, const size_t *row_off, in
                         cudaStream_t st);
 void launch_hext2h_ref(uint64_t *h, int rows, int log_m, cudaStream_t st);
 void launch_setup_to_tile(uint4 *D, const uint64_t *setup, int n, int log_m, cudaStream_t st);
+
+// kernels_out.cu: 48-byte compressed proofs, data-availability order
+void launch_g1p_compress(uint8_t *out, const uint64_t *p, size_t count, cudaStream_t st);
+void launch_h_fft_to_proofs(uint8_t *out, const uint64_t *h, int rows, int log_m, cudaStream_t st);
+void launch_tile_to_proofs(uint8_t *out, const uint4 *D, const size_t *out_off, int rows, int log_m,
+                           cudaStream_t st);
 
 // kernels_tables.cu
 size_t table_window_base_bytes();  // sizeof(G1P)

@@ -269,3 +269,42 @@ def kzg_direct(poly: np.ndarray, tau: np.ndarray, l: int = 16, j0: int = 0, j1: 
     t = np.ascontiguousarray(tau, dtype=np.uint64).reshape(4)
     lib().orc_kzg_direct(_p(out), _p(p), n, l, _p(t), j0, j1)
     return out
+
+
+# ---------------------------------------------------------------- data-availability wire format
+def g1_compress(a: np.ndarray) -> np.ndarray:
+    """48-byte compressed encodings (count, 48) uint8 of g1p_t points: x as
+    big-endian bytes with flags in the first byte -- 0x80 compressed, 0x40
+    infinity (all else zero), 0x20 when y > (p - 1) / 2 -- the BLS12-381
+    serialization of the ZCash/IETF convention (the format FK20Py's consumers
+    read; py_ecc, which FK20Py imports, is absent here)."""
+    pts = g1_normalize(np.ascontiguousarray(a, dtype=np.uint64).reshape(-1, 18))
+    out = np.zeros((pts.shape[0], 48), np.uint8)
+    for i, p in enumerate(pts):
+        if limbs_to_int(p[12:18]) == 0:
+            out[i, 0] = 0xC0
+            continue
+        x, y = limbs_to_int(p[0:6]), limbs_to_int(p[6:12])
+        b = bytearray(x.to_bytes(48, "big"))
+        b[0] |= 0x80 | (0x20 if y > (P - 1) // 2 else 0)
+        out[i] = np.frombuffer(bytes(b), np.uint8)
+    return out
+
+
+def reverse_bit_order(rows: np.ndarray) -> np.ndarray:
+    """Rows of a power-of-two length m, each permuted so that element i is the
+    original element bitrev(i) (list_to_reverse_bit_order,
+    FK20Py/kzg_proofs.py:105-118; the permutation is its own inverse)."""
+    m = rows.shape[-2] if rows.ndim >= 2 else rows.shape[0]
+    bits = m.bit_length() - 1
+    idx = [int(format(i, f"0{bits}b")[::-1], 2) for i in range(m)]
+    return rows[..., idx, :] if rows.ndim >= 2 else rows[idx]
+
+
+def da_proofs(h_fft: np.ndarray) -> np.ndarray:
+    """h_fft[rows][m] g1p_t -> proofs[rows][m][48] in data-availability order
+    (FK20Py/fk20_multi_cuda.py:249-260)."""
+    h = np.ascontiguousarray(h_fft, dtype=np.uint64)
+    rows, m = h.shape[0], h.shape[1]
+    comp = g1_compress(h.reshape(-1, 18)).reshape(rows, m, 48)
+    return reverse_bit_order(comp)

@@ -198,3 +198,29 @@ def test_fk20_degenerate_inputs():
     hb = O.fk20_row(b, xext, l)["h_fft"]
     hs = O.fk20_row(s, xext, l)["h_fft"]
     assert np.array_equal(O.g1_op("add", ha, hb), hs)
+
+
+def test_compressed_encoding_pins():
+    """The published 48-byte encoding of the BLS12-381 G1 generator (x with the
+    compression flag; its y is the smaller root), of its negation (sign flag
+    set) and of the point at infinity."""
+    g = O.g1_generator().reshape(1, 18)
+    gen = "97f1d3a73197d7942695638c4fa9ac0fc3688c4f9774b905a14e3a3f171bac586c55e83ff97a1aeffb3af00adb22c6bb"
+    assert O.g1_compress(g)[0].tobytes().hex() == gen
+    neg = O.g1_compress(O.g1_op("neg", g))[0].tobytes().hex()
+    assert neg == "b" + gen[1:]
+    inf = np.zeros((1, 18), np.uint64)
+    inf[0, 6] = 1
+    assert O.g1_compress(inf)[0].tobytes() == bytes([0xC0]) + bytes(47)
+
+
+def test_reverse_bit_order_matches_reference_definition():
+    """list_to_reverse_bit_order (kzg_proofs.py:105-118) reverses the
+    log2(m)-bit binary string of the index; applying it twice is the identity."""
+    m = 16
+    rows = np.arange(2 * m * 3).reshape(2, m, 3)
+    r = O.reverse_bit_order(rows)
+    for i in range(m):
+        j = int(('{:0' + str(m.bit_length() - 1) + 'b}').format(i)[::-1], 2)
+        assert np.array_equal(r[:, i], rows[:, j])
+    assert np.array_equal(O.reverse_bit_order(r), rows)
