@@ -57,7 +57,7 @@ def parse():
                          "micro: kernel microbenchmarks (Fp/Fr products, batched G1 FFT/IFFT, 16-term MSM)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="arrival window per load level (serve)")
     ap.add_argument("--serve-loads", default="0.5,0.9,1.2", help="offered load as fractions of plain-batch capacity")
-    ap.add_argument("--serve-max-rows", type=int, default=512)
+    ap.add_argument("--serve-max-rows", type=int, default=256)
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--autotune", action="store_true", help="ragged: autotune the context first")
     return ap.parse_args()
@@ -78,7 +78,9 @@ def workload_config(args, extra=None):
 
 
 # ------------------------------------------------------------------ distributed
-def dist_init(args):
+def dist_init(args, backend: str = "nccl"):
+    """One process per GPU (torchrun): NCCL on the GPU path; `gloo` runs the
+    same host logic on the CPU (tests)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -86,9 +88,12 @@ def dist_init(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return ws, rank, local
 
 
@@ -99,13 +104,25 @@ def barrier(ws):
 
 
 def max_over_ranks(x: float, ws: int) -> float:
+    """The step time of the job: the slowest rank's (device-timed) time."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_rows_seed(rank: int) -> int:
+    """Seed of a rank's polynomials: every rank proves its own rows (weak scaling)."""
+    return 1000 + rank
+
+
+def job_value(ws: int, proofs_per_rank: int, steps: int, total_ms: float) -> float:
+    """Whole-job proofs/s: all ranks' proofs over the slowest rank's time."""
+    return ws * proofs_per_rank * steps / (total_ms * 1e-3)
 
 
 # ------------------------------------------------------------------ clocks
@@ -223,7 +240,7 @@ def run_ours(args, ws, rank, dev):
     torch.cuda.synchronize()
     setup_s = time.time() - t0
 
-    poly_h = seeded_polys(1000 + rank, rows, n)
+    poly_h = seeded_polys(rank_rows_seed(rank), rows, n)
     poly = E.to_device(poly_h)
     h_fft = E.empty((rows, m, 18))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -253,7 +270,7 @@ def run_ours(args, ws, rank, dev):
     ctx.profile(False)
     total_ms = max_over_ranks(sum(step_ms), ws)
     clocks = clk.summary()
-    value = ws * proofs * args.steps / (total_ms * 1e-3)
+    value = job_value(ws, proofs, args.steps, total_ms)
 
     # ---- roofline of the dominant kernel kind
     imad_peak = measure_imad_peak(E, torch)
@@ -408,12 +425,12 @@ def run_serve(args, ws, rank, dev):
                 item = pending.get()
                 if item is None:
                     return
-                t, n, j, out = item
+                t, nj, j, out = item
                 done_rc.append(srv.wait(t, 120000))
                 if len(check) < 24 and j % 5 == 0:
-                    check.append((n, j % 24, out))
+                    check.append((nj, j % 24, out))
                 else:
-                    free[n].append(out)
+                    free[nj].append(out)
 
         th = threading.Thread(target=collector)
         th.start()
@@ -425,10 +442,10 @@ def run_serve(args, ws, rank, dev):
             d = due - time.perf_counter()
             if d > 0:
                 time.sleep(d)
-            n = int(lens[j])
-            out = free[n].pop() if free[n] else np.zeros((n // 8, 18), np.uint64)
-            t = srv.submit(pool[n][j % 24], out)
-            pending.put((t, n, j, out))
+            nj = int(lens[j])
+            out = free[nj].pop() if free[nj] else np.zeros((nj // 8, 18), np.uint64)
+            t = srv.submit(pool[nj][j % 24], out)
+            pending.put((t, nj, j, out))
         pending.put(None)
         th.join()
         st = srv.stats()
@@ -442,9 +459,9 @@ def run_serve(args, ws, rank, dev):
     srv.close()
     # served results are the ones the same polynomial gives alone
     same = True
-    for n, j, out in check:
-        hh = E.empty((1, n // 8, 18))
-        ctx.poly2h_fft(hh, E.to_device(pool[n][j].reshape(1, n, 4)), 1, n)
+    for nj, j, out in check:
+        hh = E.empty((1, nj // 8, 18))
+        ctx.poly2h_fft(hh, E.to_device(pool[nj][j].reshape(1, nj, 4)), 1, nj)
         same &= bool(np.array_equal(E.to_host(hh)[0], out))
     sat = max(loads, key=lambda x: x["load"])
     line = {
@@ -679,12 +696,44 @@ def run_micro(args, ws, rank, dev):
     out["msm"] = {"rows": rows, "columns": m, "terms": L, "window_bits": args.window, "ms": ms,
                   "kernel_ms": kms / kl, "achieved_gprod_s": kprod / kl / (kms / kl * 1e-3) / 1e9,
                   "frac": kprod / kl / (kms / kl * 1e-3) / peak, "bit_exact_sample": ok}
+    # ---- proofs in the data-availability wire format, straight from the tiles
+    poly = E.to_device(seeded_polys(1000, rows, n))
+    proofs = torch.zeros((rows, m, 48), dtype=torch.uint8, device="cuda")
+    h = E.empty((rows, m, 18))
+    t_h = _timed(lambda: ctx.poly2h_fft(h, poly, rows, n), 2, stream)
+    t_p = _timed(lambda: ctx.poly2proofs(proofs, poly, rows, n), 2, stream)
+    exp = O.da_proofs(O.fk20_rows(seeded_polys(1000, 1, n), E.to_host(xext)))
+    out["da_proofs"] = {"rows": rows, "n": n, "ms_h_fft": t_h, "ms_da_proofs": t_p,
+                        "proofs_per_s": rows * m / (t_p * 1e-3), "overhead": t_p / t_h - 1.0,
+                        "bit_exact_row0": bool(np.array_equal(proofs[0:1].cpu().numpy(), exp))}
     ctx.close()
+    del h, proofs
+    # ---- KZG commitments: 512 polynomials x 4096 coefficients, window 10 tables over the setup
+    cw = min(args.window, 10)
+    cctx = E.Context(dev, args.window)
+    cctx.load_commit(n, setup[:n], cw)
+    com = E.empty((rows, 18))
+    cctx.profile(True)
+    t_c = _timed(lambda: cctx.commit(com, poly, rows, n), 3, stream)
+    cms, cl, cprod = cctx.profile_read()["msm"]
+    cctx.profile(False)
+    tau = O.limbs_to_int(O.seeded_fr(1, 1)[0])
+    p0 = [O.limbs_to_int(x) for x in E.to_host(poly[0])]
+    f_tau = 0
+    for c_ in reversed(p0):
+        f_tau = (f_tau * tau + c_) % R_MOD
+    exp_c = O.g1_op("mul", O.g1_generator().reshape(1, 18), O.int_to_limbs(f_tau, 4).reshape(1, 4))
+    out["commit"] = {"rows": rows, "n": n, "window_bits": cw, "ms": t_c, "commitments_per_s": rows / (t_c * 1e-3),
+                     "achieved_gprod_s": cprod / cl / (cms / cl * 1e-3) / 1e9,
+                     "frac": cprod / cl / (cms / cl * 1e-3) / peak,
+                     "bit_exact_row0": bool(np.array_equal(O.g1_normalize(E.to_host(com[0:1])), exp_c))}
+    cctx.close()
     line = {"metric": "kernel microbenchmarks: fraction of the IMAD roofline, bit-exact samples",
-            "value": min(v["frac"] for v in out.values()), "unit": "min frac of IMAD roofline",
+            "value": min(v["frac"] for v in out.values() if "frac" in v), "unit": "min frac of IMAD roofline",
             "n_gpus": ws, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "mode": "micro", "data": "synthetic (seeded uniform residues, seeded multiples of G1)",
-            "config": {"workload": "2^24 Fp/Fr mul and sqr; 512 x 512-point G1 FFT/IFFT; 512 x 16-term MSM",
+            "config": {"workload": "2^24 Fp/Fr mul and sqr; 512 x 512-point G1 FFT/IFFT; 512 x 16-term MSM; "
+                                   "512 x 4096 proofs in the DA wire format; 512 x 4096-term commitments",
                        "imad_peak_gprod_s": peak / 1e9}, "kernels": out, "impl": "ours"}
     return line
 

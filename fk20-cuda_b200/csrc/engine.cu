@@ -321,6 +321,10 @@ struct fk20_ctx {
     int fused_occupancy = 1;    // blocks of the persistent FFT kernel that fit on one SM
     std::mutex mu;
     Tables tab[3];  // log_m 7, 8, 9
+    struct {        // KZG commitment tables over setup points s_0 .. s_{n-1}
+        DevBuf table, part;
+        int n = 0, cb = 0, W = 0;
+    } commit;
     Workspace ws;   // the context's own calls
     DevBuf D2, scratch, xext, fp_dev;
     Profiler prof;
@@ -408,23 +412,15 @@ int output_launch(Profiler &pf, uint64_t *dst, const uint4 *D, const size_t *row
     return 0;
 }
 
-int build_tables(fk20_ctx *ctx, int log_m, const uint64_t *xext, cudaStream_t st) {
-    Tables *T = tables_for(ctx, log_m);
-    const int m = 1 << log_m;
-    const int cb = ctx->window;
+// Fixed-base tables of `nbases` bases (reference g1p_t on the device) at
+// window cb, every base first multiplied by program prog_scale (< 0: none).
+int build_base_tables(fk20_ctx *ctx, DevBuf &table, const uint64_t *bases, int nbases, int cb, int prog_scale,
+                      cudaStream_t st) {
     const int W = (255 + cb - 1) / cb;
     const int E = 1 << (cb - 1);
-    const int nbases = L_COLS * m;
     const size_t entries = (size_t)nbases * W * E;
-    T->ready = false;
-    T->gen++;
-    if (xext != (const uint64_t *)T->xext.p) {  // keep the bases for rebuilds at another window
-        CKR(T->xext.reserve((size_t)L_COLS * m * sizeof(g1p_t)));
-        CK(cudaMemcpyAsync(T->xext.p, xext, (size_t)L_COLS * m * sizeof(g1p_t), cudaMemcpyDeviceToDevice, st));
-        xext = (const uint64_t *)T->xext.p;
-    }
-    T->table.release();
-    CKR(T->table.reserve(entries * 6 * sizeof(uint4)));
+    table.release();
+    CKR(table.reserve(entries * 6 * sizeof(uint4)));
     // slabs of bases keep the Z scratch near 1 GiB
     const size_t per_base_z = (size_t)W * E * table_z_bytes();
     int slab = (int)std::max<size_t>(1, (1ull << 30) / per_base_z);
@@ -434,13 +430,30 @@ int build_tables(fk20_ctx *ctx, int log_m, const uint64_t *xext, cudaStream_t st
     void *wb = (char *)ctx->scratch.p + (size_t)slab * per_base_z;
     for (int b0 = 0; b0 < nbases; b0 += slab) {
         const int nb = std::min(slab, nbases - b0);
-        launch_table_windows(wb, xext, b0, nb, W, cb, 512 + log_m, st);
+        launch_table_windows(wb, bases, b0, nb, W, cb, prog_scale, st);
         CKL();
-        launch_table_fill((uint4 *)T->table.p, zs, wb, b0, nb, W, cb, st);
+        launch_table_fill((uint4 *)table.p, zs, wb, b0, nb, W, cb, st);
         CKL();
-        launch_table_affine((uint4 *)T->table.p, zs, b0, nb, W, cb, st);
+        launch_table_affine((uint4 *)table.p, zs, b0, nb, W, cb, st);
         CKL();
     }
+    return 0;
+}
+
+int build_tables(fk20_ctx *ctx, int log_m, const uint64_t *xext, cudaStream_t st) {
+    Tables *T = tables_for(ctx, log_m);
+    const int m = 1 << log_m;
+    const int cb = ctx->window;
+    const int W = (255 + cb - 1) / cb;
+    T->ready = false;
+    T->gen++;
+    if (xext != (const uint64_t *)T->xext.p) {  // keep the bases for rebuilds at another window
+        CKR(T->xext.reserve((size_t)L_COLS * m * sizeof(g1p_t)));
+        CK(cudaMemcpyAsync(T->xext.p, xext, (size_t)L_COLS * m * sizeof(g1p_t), cudaMemcpyDeviceToDevice, st));
+        xext = (const uint64_t *)T->xext.p;
+    }
+    // the inverse FFT's 1/m folded into the bases (program 512 + log m = 2^-log m)
+    CKR(build_base_tables(ctx, T->table, xext, L_COLS * m, cb, 512 + log_m, st));
     T->n = (unsigned)(m * L_COLS / 2);
     T->log_m = log_m;
     T->cb = cb;
@@ -488,6 +501,9 @@ struct Seg {
 };
 
 constexpr size_t SYNC_HDR = 256;  // persistent-launch header: task counter at 0, error flag at 128
+// Fp products per compressed proof: inversion by Fermat (381 squarings + 190
+// products), two products to affine, two conversions out of Montgomery form
+constexpr double PROOF_OUT_MP = 575.0;
 
 struct SegLayout {
     size_t s_off[MAX_SEGS], d_off[MAX_SEGS], r_off[MAX_SEGS];
@@ -529,8 +545,8 @@ int reserve_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, bool
 // outputs; or (!full) the hext_fft outputs times m.  The tables are the
 // context's; the workspace is the caller's.  Allocates only when `ws` is too
 // small (reserve_segments first makes the enqueue allocation-free).
-int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr_t *polys, g1p_t *out, bool full,
-                 cudaStream_t st) {
+int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr_t *polys, void *out, bool full,
+                 cudaStream_t st, bool proofs = false, int fft_bps = 0) {
     SegLayout lay;
     CKR(segment_layout(ctx, sg, nseg, lay));
     CKR(reserve_segments(ctx, ws, sg, nseg, full));
@@ -582,8 +598,10 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
         p.next = (unsigned *)ws.sync.p;
         p.err = (int *)((char *)ws.sync.p + 128);
         p.epoch = 1;  // counters are cleared before every launch
+        // persistent grid: the context's setting, or the caller's share of the SMs (server packs)
         int per_sm = ctx->fused_occupancy;
-        if (ctx->fft_blocks_per_sm > 0 && ctx->fft_blocks_per_sm < per_sm) per_sm = ctx->fft_blocks_per_sm;
+        const int want = fft_bps > 0 ? fft_bps : ctx->fft_blocks_per_sm;
+        if (want > 0 && want < per_sm) per_sm = want;
         const unsigned max_blocks = (widest + FFT_WARPS - 1) / FFT_WARPS;
         p.blocks = (int)std::min<unsigned>((unsigned)(ctx->sms * per_sm), max_blocks);
         CK(cudaMemsetAsync(ws.sync.p, 0, SYNC_HDR + lay.r_bytes, st));
@@ -597,9 +615,18 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
             CKR(run_hext_to_hfft(ctx->prof, D + lay.d_off[k] / U, (int)((sg[k].rows + 31) / 32), (int)sg[k].rows,
                                  sg[k].log_m, 0, st));
     }
-    for (int k = 0; k < nseg; k++)
-        CKR(output_launch(ctx->prof, (uint64_t *)out, D + lay.d_off[k] / U, sg[k].out_off, (int)sg[k].rows,
-                          sg[k].log_m, 0, st));
+    for (int k = 0; k < nseg; k++) {
+        if (proofs) {  // compressed, data-availability order (kernels_out.cu)
+            ctx->prof.begin(FK20_K_OUTPUT, (double)sg[k].rows * (1 << sg[k].log_m) * PROOF_OUT_MP * MP, st);
+            launch_tile_to_proofs((uint8_t *)out, D + lay.d_off[k] / U, sg[k].out_off, (int)sg[k].rows,
+                                  sg[k].log_m, st);
+            ctx->prof.end(st);
+            CKL();
+        } else {
+            CKR(output_launch(ctx->prof, (uint64_t *)out, D + lay.d_off[k] / U, sg[k].out_off, (int)sg[k].rows,
+                              sg[k].log_m, 0, st));
+        }
+    }
     return 0;
 }
 
@@ -799,6 +826,8 @@ int fk20_ctx_destroy(fk20_ctx *ctx) {
         DeviceGuard dg(ctx->device);
         cudaDeviceSynchronize();
         for (auto &t : ctx->tab) t.table.release(), t.xext.release();
+        ctx->commit.table.release();
+        ctx->commit.part.release();
         ctx->ws.release();
         ctx->D2.release();
         ctx->scratch.release();
@@ -841,6 +870,7 @@ size_t fk20_ctx_device_bytes(const fk20_ctx *ctx) {
     if (!ctx) return 0;
     size_t b = ctx->ws.bytes() + ctx->D2.bytes + ctx->scratch.bytes + ctx->xext.bytes;
     for (auto &t : ctx->tab) b += t.table.bytes + t.xext.bytes;
+    b += ctx->commit.table.bytes + ctx->commit.part.bytes;
     return b;
 }
 
@@ -1172,6 +1202,87 @@ int fk20_ctx_autotune(fk20_ctx *ctx, unsigned n, unsigned rows, size_t max_table
     return autotune(ctx, log_m, rows, max_table_bytes, result, S_(stream));
 }
 
+// ---------------------------------------------------------------- KZG commitments
+int fk20_ctx_load_commit(fk20_ctx *ctx, unsigned n, const g1p_t *setup, int window, void *stream) {
+    if (!ctx || !setup || n == 0 || n % COMMIT_CHUNK || n > (1u << 16)) return FK20_EINVAL;
+    if (window == 0) window = 10;
+    if (window < 8 || window > 13) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    cudaStream_t st = S_(stream);
+    ctx->commit.n = 0;
+    CKR(build_base_tables(ctx, ctx->commit.table, (const uint64_t *)setup, (int)n, window, -1, st));
+    CK(cudaStreamSynchronize(st));
+    ctx->commit.cb = window;
+    ctx->commit.W = (255 + window - 1) / window;
+    ctx->commit.n = (int)n;
+    return 0;
+}
+
+int fk20_ctx_commit(fk20_ctx *ctx, g1p_t *commitment, const fr_t *polynomial, unsigned rows, unsigned n,
+                    void *stream) {
+    if (!ctx) return FK20_EINVAL;
+    CKR(check_call(commitment, polynomial, rows));
+    if (n == 0 || n % COMMIT_CHUNK) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    if (!ctx->commit.n || (int)n > ctx->commit.n) return FK20_ENOSETUP;
+    const int G = (int)((rows + 31) / 32);
+    CKR(ctx->commit.part.reserve(tile_bytes(G, (int)(n / COMMIT_CHUNK))));
+    const double prod = (double)rows * n * ctx->commit.W * MADD_P + (double)rows * (n / COMMIT_CHUNK) * ADD_P;
+    ctx->prof.begin(FK20_K_MSM, prod, S_(stream));
+    launch_commit((uint64_t *)commitment, (uint4 *)ctx->commit.part.p, (const uint64_t *)polynomial,
+                  (const uint4 *)ctx->commit.table.p, (int)rows, (int)n, ctx->commit.W, ctx->commit.cb, S_(stream));
+    ctx->prof.end(S_(stream));
+    CKL();
+    return 0;
+}
+
+// ---------------------------------------------------------------- data-availability output
+int fk20_g1p_compress_n(uint8_t *out, const g1p_t *p, size_t count, void *stream) {
+    if (!out || !p || count == 0 || (((uintptr_t)out | (uintptr_t)p) & 15)) return FK20_EINVAL;
+    CKR(current_device_ready());
+    launch_g1p_compress(out, (const uint64_t *)p, count, S_(stream));
+    CKL();
+    return 0;
+}
+
+int fk20_h_fft2proofs(uint8_t *proofs, const g1p_t *h_fft, unsigned rows, unsigned n, void *stream) {
+    const int log_m = log_m_for_n(n);
+    if (log_m < 0) return FK20_EINVAL;
+    CKR(check_call(proofs, h_fft, rows));
+    CKR(current_device_ready());
+    launch_h_fft_to_proofs(proofs, (const uint64_t *)h_fft, (int)rows, log_m, S_(stream));
+    CKL();
+    return 0;
+}
+
+int fk20_ctx_poly2proofs(fk20_ctx *ctx, uint8_t *proofs, const fr_t *polynomial, unsigned rows, unsigned n,
+                         void *stream) {
+    if (!ctx) return FK20_EINVAL;
+    CKR(check_call(proofs, polynomial, rows));
+    const int log_m = log_m_for_n(n);
+    if (log_m < 0) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    if (!tables_for(ctx, log_m)->ready) return FK20_ENOSETUP;
+    const Seg sg{log_m, rows, nullptr, nullptr};
+    return run_segments(ctx, ctx->ws, &sg, 1, polynomial, proofs, true, S_(stream), true);
+}
+
+int fk20_ctx_batch_proofs(fk20_ctx *ctx, uint8_t *proofs, const fr_t *polys, unsigned count, const unsigned *n,
+                          const size_t *poly_off, const size_t *out_off, void *stream) {
+    if (!ctx) return FK20_EINVAL;
+    CKR(check_batch((const g1p_t *)proofs, polys, count, n, poly_off, out_off));
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    cudaStream_t st = S_(stream);
+    Seg sg[3];
+    int nseg = 0;
+    CKR(batch_segments(ctx, ctx->ws, count, n, poly_off, out_off, sg, &nseg, st));
+    return run_segments(ctx, ctx->ws, sg, nseg, polys, proofs, true, st, true);
+}
+
 // ---------------------------------------------------------------- reference entry points
 int fk20_poly2h_fft(g1p_t *h_fft, const fr_t *polynomial, const g1p_t *xext_fft, unsigned rows) {
     if (!xext_fft) return FK20_EINVAL;
@@ -1480,7 +1591,11 @@ int enqueue_pack(fk20_server *s, Slot &sl) {
         Seg sg[3];
         int nseg = 0;
         CKR(batch_segments(ctx, sl.ws, (unsigned)cnt, ns.data(), poly_off.data(), out_off.data(), sg, &nseg, sl.st));
-        CKR(run_segments(ctx, sl.ws, sg, nseg, (const fr_t *)sl.dpoly.p, (g1p_t *)sl.dout.p, true, sl.st));
+        // each pack's persistent FFT takes a share of the SMs, so packs of
+        // different slots run side by side instead of one after the other
+        const int share = std::max(1, ctx->fused_occupancy / (int)s->slots.size());
+        CKR(run_segments(ctx, sl.ws, sg, nseg, (const fr_t *)sl.dpoly.p, (g1p_t *)sl.dout.p, true, sl.st, false,
+                         share));
     }
     CK(cudaMemcpyAsync(sl.hout, sl.dout.p, out * sizeof(g1p_t), cudaMemcpyDeviceToHost, sl.st));
     CK(cudaLaunchHostFunc(sl.st, pack_done_cb, s));
@@ -1628,7 +1743,7 @@ extern "C" {
 int fk20_server_create(fk20_server **out, fk20_ctx *ctx, const fk20_server_config *cfg) {
     if (!out || !ctx) return FK20_EINVAL;
     fk20_server_config c = cfg ? *cfg : fk20_server_config{};
-    if (!c.max_rows) c.max_rows = 512;
+    if (!c.max_rows) c.max_rows = 256;
     if (!c.slots) c.slots = 2;
     if (!c.max_queue) c.max_queue = 1u << 16;
     if (c.max_rows > 4096 || c.slots > 8) return FK20_EINVAL;
@@ -1647,10 +1762,40 @@ int fk20_server_create(fk20_server **out, fk20_ctx *ctx, const fk20_server_confi
         }
         s->slots.resize(c.slots);
         int rc = 0;
+        // Size every slot for a full pack now (max_rows requests of the longest
+        // length, plus a partial group per length) when that fits the budget:
+        // growing a buffer later would synchronise the device and stall the
+        // other slots' packs.
+        const unsigned full[3] = {32, 32, c.max_rows + 32};
+        const bool presize = pack_bytes(full) * c.slots <= c.hbm_budget;
         for (Slot &sl : s->slots) {
             if (!rc && cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) != cudaSuccess) rc = (int)cudaGetLastError();
             if (!rc && cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) rc = (int)cudaGetLastError();
             if (!rc) rc = sl.ws.init();
+            if (!rc && presize) {
+                const size_t in_b = (size_t)(c.max_rows + 64) * 4096 * sizeof(fr_t);
+                const size_t out_b = (size_t)(c.max_rows + 64) * 512 * sizeof(g1p_t);
+                const Seg sg[3] = {{7, 32, nullptr, nullptr}, {8, 32, nullptr, nullptr},
+                                   {9, c.max_rows + 32, nullptr, nullptr}};
+                rc = sl.dpoly.reserve(in_b);
+                if (!rc) rc = sl.dout.reserve(out_b);
+                if (!rc) rc = pinned_reserve(&sl.hpoly, &sl.hpoly_bytes, in_b);
+                if (!rc) rc = pinned_reserve(&sl.hout, &sl.hout_bytes, out_b);
+                if (!rc) rc = sl.ws.stage_offsets(2 * (size_t)(c.max_rows + 64));
+                if (!rc) rc = sl.ws.offs.reserve(2 * (size_t)(c.max_rows + 64) * sizeof(size_t));
+                if (!rc) {
+                    SegLayout lay;
+                    for (int k = 0; k < 3 && !rc; k++) {
+                        const int m = 1 << sg[k].log_m, G = (int)((sg[k].rows + 31) / 32);
+                        lay.s_bytes += scal_bytes(G, m);
+                        lay.d_bytes += tile_bytes(G, m);
+                        lay.r_bytes += (size_t)G * m * sizeof(unsigned);
+                    }
+                    rc = sl.ws.S.reserve(lay.s_bytes);
+                    if (!rc) rc = sl.ws.D.reserve(lay.d_bytes);
+                    if (!rc) rc = sl.ws.sync.reserve(SYNC_HDR + lay.r_bytes);
+                }
+            }
         }
         if (rc) {
             server_free(s);

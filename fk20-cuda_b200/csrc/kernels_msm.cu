@@ -25,6 +25,42 @@ namespace fk {
 
 cudaError_t upload_consts_msm() { return upload_module_consts(); }
 
+// acc += s * X for one base X, whose table `tb` holds (e+1) 2^(cb w) X for
+// window w and e < 2^(cb-1): the 255-bit scalar s (9 words, s[8] = 0) is
+// recoded into W signed digits in [-2^(cb-1), 2^(cb-1)] on the fly and every
+// nonzero digit costs one mixed addition of a gathered 96-byte entry.
+FK_D void msm_add_scalar(G1P &acc, const uint32_t s[9], const uint4 *__restrict__ tb, int W, int cb) {
+    const int E = 1 << (cb - 1);
+    const uint32_t mask = (1u << cb) - 1u;
+    int carry = 0;
+    for (int w = 0; w < W; w++) {
+        const int bit = w * cb;
+        const int wd = bit >> 5, sh = bit & 31;
+        uint32_t raw = s[wd] >> sh;
+        if (sh + cb > 32) raw |= s[wd + 1] << (32 - sh);
+        int d = (int)(raw & mask) + carry;
+        carry = d > E;
+        if (carry) d -= (1 << cb);
+        if (d != 0) {
+            const int e = (d < 0 ? -d : d) - 1;
+            const uint4 *ent = tb + ((size_t)w * E + e) * 6;
+            Fp x, y;
+            const uint4 q0 = ent[0], q1 = ent[1], q2 = ent[2], q3 = ent[3], q4 = ent[4], q5 = ent[5];
+            x.w[0] = q0.x; x.w[1] = q0.y; x.w[2] = q0.z; x.w[3] = q0.w;
+            x.w[4] = q1.x; x.w[5] = q1.y; x.w[6] = q1.z; x.w[7] = q1.w;
+            x.w[8] = q2.x; x.w[9] = q2.y; x.w[10] = q2.z; x.w[11] = q2.w;
+            y.w[0] = q3.x; y.w[1] = q3.y; y.w[2] = q3.z; y.w[3] = q3.w;
+            y.w[4] = q4.x; y.w[5] = q4.y; y.w[6] = q4.z; y.w[7] = q4.w;
+            y.w[8] = q5.x; y.w[9] = q5.y; y.w[10] = q5.z; y.w[11] = q5.w;
+            // an entry (0, 0) encodes a base at infinity (not on the curve)
+            if (!(f_is_zero(x) && f_is_zero(y))) {
+                if (d < 0) f_neg(y, y);
+                g1_madd(acc, acc, x, y);
+            }
+        }
+    }
+}
+
 // One warp per (segment, column c, group g of 32 rows); lanes are rows.
 // Warps are numbered segment by segment, g fastest, so the warps of a block
 // read the same table column.
@@ -41,7 +77,6 @@ __global__ void __launch_bounds__(MSM_MAX_THREADS, FK_MSM_MINB) k_msm(const __gr
     const int row = g * 32 + lane;
     const bool live = row < a.rows;
     const int E = 1 << (a.cb - 1);
-    const uint32_t mask = (1u << a.cb) - 1u;
     G1P acc;
     g1_set_inf(acc);
     for (int i = 0; i < L_COLS; i++) {
@@ -56,38 +91,64 @@ __global__ void __launch_bounds__(MSM_MAX_THREADS, FK_MSM_MINB) k_msm(const __gr
             for (int k = 0; k < 9; k++) s[k] = 0;
         }
         const uint4 *tb = a.table + ((size_t)(i * m + c) * a.W) * E * 6;
-        int carry = 0;
-        for (int w = 0; w < a.W; w++) {
-            const int bit = w * a.cb;
-            const int wd = bit >> 5, sh = bit & 31;
-            uint32_t raw = s[wd] >> sh;
-            if (sh + a.cb > 32) raw |= s[wd + 1] << (32 - sh);
-            int d = (int)(raw & mask) + carry;
-            carry = d > E;
-            if (carry) d -= (1 << a.cb);
-            if (d != 0) {
-                const int e = (d < 0 ? -d : d) - 1;
-                const uint4 *ent = tb + ((size_t)w * E + e) * 6;
-                Fp x, y;
-                const uint4 q0 = ent[0], q1 = ent[1], q2 = ent[2], q3 = ent[3], q4 = ent[4], q5 = ent[5];
-                x.w[0] = q0.x; x.w[1] = q0.y; x.w[2] = q0.z; x.w[3] = q0.w;
-                x.w[4] = q1.x; x.w[5] = q1.y; x.w[6] = q1.z; x.w[7] = q1.w;
-                x.w[8] = q2.x; x.w[9] = q2.y; x.w[10] = q2.z; x.w[11] = q2.w;
-                y.w[0] = q3.x; y.w[1] = q3.y; y.w[2] = q3.z; y.w[3] = q3.w;
-                y.w[4] = q4.x; y.w[5] = q4.y; y.w[6] = q4.z; y.w[7] = q4.w;
-                y.w[8] = q5.x; y.w[9] = q5.y; y.w[10] = q5.z; y.w[11] = q5.w;
-                // an entry (0, 0) encodes a base at infinity (not on the curve)
-                if (!(f_is_zero(x) && f_is_zero(y))) {
-                    if (d < 0) f_neg(y, y);
-                    g1_madd(acc, acc, x, y);
-                }
-            }
-        }
+        msm_add_scalar(acc, s, tb, a.W, a.cb);
     }
     if (args.times_m) {
         for (int t = 0; t < a.log_m; t++) g1_dbl(acc, acc);
     }
     tile_store(a.D + tile_index(g, m, c), lane, acc);
+}
+
+// ---------------------------------------------------------------- KZG commitments
+// commitment[row] = sum_i poly[row][i] * s_i over fixed-base tables of the
+// setup points s_i (commit_to_poly, FK20Py/kzg_proofs.py:159-163).  Pass 1:
+// warp (g, chunk) sums the COMMIT_CHUNK bases of its chunk for 32 rows into a
+// partial-sum tile; pass 2: one thread per row adds its chunks' partials.
+__global__ void __launch_bounds__(128) k_commit_partial(uint4 *__restrict__ part, const uint64_t *__restrict__ poly,
+                                                        const uint4 *__restrict__ table, int rows, int n, int W,
+                                                        int cb) {
+    const int chunks = n / COMMIT_CHUNK;
+    const int G = (rows + 31) / 32;
+    const unsigned warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (warp >= (unsigned)G * chunks) return;
+    const int lane = threadIdx.x & 31;
+    const int g = (int)(warp % (unsigned)G), c = (int)(warp / (unsigned)G);
+    const int row = g * 32 + lane;
+    const bool live = row < rows;
+    const int E = 1 << (cb - 1);
+    G1P acc;
+    g1_set_inf(acc);
+    for (int i = c * COMMIT_CHUNK; i < (c + 1) * COMMIT_CHUNK; i++) {
+        uint32_t s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (live) {
+            Fr f;
+            fr_from_ref(f, poly + 4 * ((size_t)row * n + i));
+#pragma unroll
+            for (int k = 0; k < 8; k++) s[k] = f.w[k];
+        }
+        msm_add_scalar(acc, s, table + (size_t)i * W * E * 6, W, cb);
+    }
+    tile_store(part + tile_index(g, chunks, c), lane, acc);
+}
+
+__global__ void k_commit_reduce(uint64_t *__restrict__ out, const uint4 *__restrict__ part, int rows, int chunks) {
+    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
+        const int g = row >> 5, lane = row & 31;
+        G1P acc, q;
+        tile_load(acc, part + tile_index(g, chunks, 0), lane);
+        for (int c = 1; c < chunks; c++) {
+            tile_load(q, part + tile_index(g, chunks, c), lane);
+            g1_add(acc, acc, q);
+        }
+        g1p_to_ref(out + 18 * (size_t)row, acc);
+    }
+}
+
+void launch_commit(uint64_t *out, uint4 *part, const uint64_t *poly, const uint4 *table, int rows, int n, int W,
+                   int cb, cudaStream_t st) {
+    const unsigned warps = (unsigned)((rows + 31) / 32) * (unsigned)(n / COMMIT_CHUNK);
+    k_commit_partial<<<blocks_for(warps, 4), 128, 0, st>>>(part, poly, table, rows, n, W, cb);
+    k_commit_reduce<<<blocks_for((size_t)rows, 128), 128, 0, st>>>(out, part, rows, n / COMMIT_CHUNK);
 }
 
 void launch_msm(const MsmArgs &a, int threads, cudaStream_t st) {

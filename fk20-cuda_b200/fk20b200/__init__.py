@@ -39,6 +39,8 @@ ABI_SYMBOLS = (
     "fk20_ctx_set", "fk20_ctx_status", "g1p_fft_noalloc", "fk20_ctx_get", "fk20_plan_create",
     "fk20_plan_launch", "fk20_plan_destroy", "fk20_ctx_autotune", "fk20_server_create", "fk20_server_submit",
     "fk20_server_wait", "fk20_server_get_stats", "fk20_server_reset_stats", "fk20_server_destroy",
+    "fk20_g1p_compress_n", "fk20_h_fft2proofs", "fk20_ctx_poly2proofs", "fk20_ctx_batch_proofs",
+    "fk20_ctx_load_commit", "fk20_ctx_commit",
 )
 
 # kernel kinds of the per-launch profiler (FK20_K_* in the header)
@@ -146,6 +148,12 @@ def lib() -> ctypes.CDLL:
             "fk20_server_get_stats": ([vp, ctypes.POINTER(ServerStats)], i),
             "fk20_server_reset_stats": ([vp], i),
             "fk20_server_destroy": ([vp], i),
+            "fk20_g1p_compress_n": ([vp, vp, sz, vp], i),
+            "fk20_h_fft2proofs": ([vp, vp, u, u, vp], i),
+            "fk20_ctx_poly2proofs": ([vp, vp, vp, u, u, vp], i),
+            "fk20_ctx_batch_proofs": ([vp, vp, vp, u, vp, vp, vp, vp], i),
+            "fk20_ctx_load_commit": ([vp, u, vp, i, vp], i),
+            "fk20_ctx_commit": ([vp, vp, vp, u, u, vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -223,6 +231,22 @@ class Context:
 
     def poly2hext_fft(self, hext_fft, poly, rows: int, n: int):
         call("fk20_ctx_poly2hext_fft", self.h, _ptr(hext_fft), _ptr(poly), rows, n, _stream())
+
+    def load_commit(self, n: int, setup, window: int = 0):
+        call("fk20_ctx_load_commit", self.h, n, _ptr(setup), window, _stream())
+
+    def commit(self, commitments, poly, rows: int, n: int):
+        """commitments[rows] (g1p_t) = sum_i poly[row][i] * setup_i."""
+        call("fk20_ctx_commit", self.h, _ptr(commitments), _ptr(poly), rows, n, _stream())
+
+    def poly2proofs(self, proofs, poly, rows: int, n: int):
+        """proofs: uint8 CUDA tensor [rows][2n/16][48], data-availability order."""
+        call("fk20_ctx_poly2proofs", self.h, _ptr(proofs), _ptr(poly), rows, n, _stream())
+
+    def batch_proofs(self, proofs, polys, ns, poly_off, out_off):
+        cnt = len(ns)
+        call("fk20_ctx_batch_proofs", self.h, _ptr(proofs), _ptr(polys), cnt, (ctypes.c_uint * cnt)(*ns),
+             (ctypes.c_size_t * cnt)(*poly_off), (ctypes.c_size_t * cnt)(*out_off), _stream())
 
     def msm(self, hext_fft, tc_fft, rows: int, n: int):
         call("fk20_ctx_msm", self.h, _ptr(hext_fft), _ptr(tc_fft), rows, n, _stream())

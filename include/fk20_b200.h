@@ -171,6 +171,41 @@ int fk20_ctx_profile_read(fk20_ctx *ctx, int kind, double *ms, long *launches, d
  * w_512^index; 512 + s: 2^-s), for work accounting. */
 int fk20_program_cost(int index, int *dbl, int *add);
 
+/* ------------------------------------------------------------------ KZG commitments
+ * commitment[r] = sum_i polynomial[r][i] * s_i, the commitment of
+ * commit_to_poly (FK20Py/kzg_proofs.py:159-163; no CUDA counterpart in the
+ * reference), as a fixed-base MSM over tables of the setup points s_0..s_{n-1}:
+ * fk20_ctx_load_commit builds them (window 8..13, 0 = 10; n a multiple of 32,
+ * at most 65536: 4096 points at window 10 take 5.2 GB), fk20_ctx_commit
+ * commits rows polynomials of n' <= n coefficients (n' a multiple of 32). */
+int fk20_ctx_load_commit(fk20_ctx *ctx, unsigned n, const g1p_t *setup, int window, void *stream);
+int fk20_ctx_commit(fk20_ctx *ctx, g1p_t *commitment, const fr_t *polynomial, unsigned rows, unsigned n,
+                    void *stream);
+
+/* ------------------------------------------------------------------ data-availability output
+ * Proofs as data-availability consumers read them (no CUDA counterpart in the
+ * reference; the Python path is FK20Py/fk20_multi_cuda.py:249-260 with
+ * list_to_reverse_bit_order, FK20Py/kzg_proofs.py:105-118): each proof is the
+ * 48-byte compressed encoding of its affine point -- x big-endian, flag bits
+ * 0x80 compressed, 0x40 infinity, 0x20 y > (p-1)/2 in the first byte -- and the
+ * m proofs of a row are in bit-reversed order: proof i of a row is
+ * h_fft[bitrev(i)].  Output buffers are DEVICE bytes, 16-byte aligned. */
+
+/* out[count][48] = compressed encodings of p[count] (natural order) */
+int fk20_g1p_compress_n(uint8_t *out, const g1p_t *p, size_t count, void *stream);
+
+/* h_fft[rows][m] -> proofs[rows][m][48] in data-availability order */
+int fk20_h_fft2proofs(uint8_t *proofs, const g1p_t *h_fft, unsigned rows, unsigned n, void *stream);
+
+/* The whole pipeline with this output written straight from the engine's
+ * tiles: polynomial[rows][n] -> proofs[rows][m][48]. */
+int fk20_ctx_poly2proofs(fk20_ctx *ctx, uint8_t *proofs, const fr_t *polynomial, unsigned rows, unsigned n,
+                         void *stream);
+
+/* Ragged batch (as fk20_ctx_batch) with this output; out_off[j] counts proofs. */
+int fk20_ctx_batch_proofs(fk20_ctx *ctx, uint8_t *proofs, const fr_t *polys, unsigned count, const unsigned *n,
+                          const size_t *poly_off, const size_t *out_off, void *stream);
+
 /* ------------------------------------------------------------------ request server
  * Continuous batching of blob-proof requests (no reference counterpart: the
  * reference has no serving layer).  A worker thread admits requests as they
@@ -180,14 +215,16 @@ int fk20_program_cost(int index, int *dbl, int *add);
  * waiting than a pack takes -- up to max_rows and the device-memory budget,
  * and enqueues them as one segment pipeline (one MSM launch and one
  * persistent G1 FFT launch over all lengths).  Packs of different slots
- * overlap on the device; requests that arrive meanwhile wait for the next
- * free slot.  The setup tables stay resident in the context (load every
+ * run side by side on the device (each pack's persistent FFT takes a share
+ * of the SMs); requests that arrive meanwhile wait for the next free slot.
+ * Slot buffers are sized for a full pack at creation when that fits the
+ * budget.  The setup tables stay resident in the context (load every
  * length the requests use first).  Each request's result is the same as a
  * fk20_ctx_poly2h_fft of that polynomial alone.
  */
 typedef struct fk20_server fk20_server;
 typedef struct {
-    unsigned max_rows;  /* requests per pack (1..4096; 0 = 512) */
+    unsigned max_rows;  /* requests per pack (1..4096; 0 = 256) */
     unsigned slots;     /* packs in flight at once (1..8; 0 = 2) */
     size_t hbm_budget;  /* device bytes all slots' buffers may hold (0 = half the free memory at creation) */
     unsigned max_queue; /* waiting requests beyond which submit returns FK20_EAGAIN (0 = 1 << 16) */
