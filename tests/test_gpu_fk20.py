@@ -361,3 +361,19 @@ def test_autotune_keeps_results(engine):
     assert _eq_count(engine, before, after) == (rows * m, rows * m)
     assert c.status() == 0
     c.close()
+
+
+@pytest.mark.parametrize("rows", [1, 31, 33, 577])
+def test_row_counts_around_group_boundaries(engine, rows):
+    """Partial 32-row groups (idle lanes) at small and large row counts:
+    sampled proofs of the first, last and a middle row against the KZG
+    identity [q_j(tau)] G1."""
+    n, m = 4096, 512
+    tau, _, _ = fk20_setup_data(n)
+    poly = O.seeded_fr(7000 + rows, rows * n).reshape(rows, n, 4)
+    h = engine.empty((rows, m, 18))
+    ctx_for(engine, n).poly2h_fft(h, engine.to_device(poly), rows, n)
+    got = engine.to_host(h)
+    for r, j in [(0, 3), (rows - 1, 509), (rows // 2, 256)]:
+        direct = O.kzg_direct(poly[r], tau, 16, j, j + 1)[0]
+        assert np.array_equal(O.g1_normalize(got[r, j]), direct), (rows, r, j)

@@ -75,3 +75,19 @@ def test_server_without_tables_for_a_length(engine):
     assert e.value.code == engine.FK20_ENOSETUP
     srv.close()
     c.close()
+
+
+def test_server_close_finishes_pending_requests(engine, served_ctx):
+    """Closing the server completes every request already submitted."""
+    sizes = [1024, 4096, 2048] * 7
+    polys = [O.seeded_fr(4500 + j, n) for j, n in enumerate(sizes)]
+    outs = [np.zeros((n // 8, 18), np.uint64) for n in sizes]
+    srv = engine.Server(served_ctx, max_rows=8, slots=2)
+    for j in range(len(sizes)):
+        srv.submit(polys[j], outs[j])
+    srv.close()  # returns once the worker has written every result
+    for j in (0, 10, len(sizes) - 1):
+        n = sizes[j]
+        h = engine.empty((1, n // 8, 18))
+        served_ctx.poly2h_fft(h, engine.to_device(polys[j].reshape(1, n, 4)), 1, n)
+        assert np.array_equal(engine.to_host(h)[0], outs[j]), j
