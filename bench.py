@@ -253,7 +253,10 @@ def gpu_eq(E, a, b) -> bool:
     import torch
     cnt = a.numel() // 18
     eq = torch.zeros(cnt, dtype=torch.uint8, device="cuda")
-    E.call("g1p_eq_n", E._ptr(eq), E._ptr(a.contiguous()), E._ptr(b.contiguous()), cnt, E._stream())
+    # operands bound to names: a temporary passed only through its address
+    # could be freed, and its memory reused, before the kernel reads it
+    ac, bc = a.contiguous(), b.contiguous()
+    E.call("g1p_eq_n", E._ptr(eq), E._ptr(ac), E._ptr(bc), cnt, E._stream())
     return int(eq.sum()) == cnt
 
 
@@ -746,12 +749,12 @@ def run_micro(args, ws, rank, dev):
     for r in (0, rows - 1):
         for c in range(4):
             terms = E.empty((L, 18))
-            E.call("g1p_op_n", E.G1_OPS["mul"], E._ptr(terms), E._ptr(xext[:, c].contiguous()),
-                   E._ptr(dtc[r, :, c].contiguous()), L, E._stream())
+            bases, scalars = xext[:, c].contiguous(), dtc[r, :, c].contiguous()
+            E.call("g1p_op_n", E.G1_OPS["mul"], E._ptr(terms), E._ptr(bases), E._ptr(scalars), L, E._stream())
             acc = terms[0:1].clone()
             for i in range(1, L):
-                E.call("g1p_op_n", E.G1_OPS["add"], E._ptr(acc), E._ptr(acc), E._ptr(terms[i:i + 1].contiguous()), 1,
-                       E._stream())
+                term = terms[i:i + 1]
+                E.call("g1p_op_n", E.G1_OPS["add"], E._ptr(acc), E._ptr(acc), E._ptr(term), 1, E._stream())
             ok &= gpu_eq(E, acc, hext[r, c:c + 1])
     out["msm"] = {"rows": rows, "columns": m, "terms": L, "window_bits": args.window, "ms": ms,
                   "kernel_ms": kms / kl, "achieved_gprod_s": kprod / kl / (kms / kl * 1e-3) / 1e9,
@@ -784,8 +787,8 @@ def run_micro(args, ws, rank, dev):
     for c_ in reversed(p0):
         f_tau = (f_tau * tau + c_) % R_MOD
     exp_c = E.empty((1, 18))
-    E.call("g1p_op_n", E.G1_OPS["mul"], E._ptr(exp_c), E._ptr(E.to_device(g1_generator().reshape(1, 18))),
-           E._ptr(E.to_device(int_to_limbs(f_tau, 4).reshape(1, 4))), 1, E._stream())
+    dgen, dft = E.to_device(g1_generator().reshape(1, 18)), E.to_device(int_to_limbs(f_tau, 4).reshape(1, 4))
+    E.call("g1p_op_n", E.G1_OPS["mul"], E._ptr(exp_c), E._ptr(dgen), E._ptr(dft), 1, E._stream())
     out["commit"] = {"rows": rows, "n": n, "window_bits": cw, "ms": t_c, "commitments_per_s": rows / (t_c * 1e-3),
                      "achieved_gprod_s": cprod / cl / (cms / cl * 1e-3) / 1e9,
                      "frac": cprod / cl / (cms / cl * 1e-3) / peak,
