@@ -57,7 +57,7 @@ def parse():
                          "micro: kernel microbenchmarks (Fp/Fr products, batched G1 FFT/IFFT, 16-term MSM)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="arrival window per load level (serve)")
     ap.add_argument("--serve-loads", default="0.5,0.9,1.2", help="offered load as fractions of plain-batch capacity")
-    ap.add_argument("--serve-max-rows", type=int, default=256)
+    ap.add_argument("--serve-max-rows", type=int, default=160)
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--autotune", action="store_true", help="ragged: autotune the context first")
     return ap.parse_args()

@@ -1110,6 +1110,17 @@ int autotune(fk20_ctx *ctx, int log_m, unsigned rows, size_t max_table_bytes, fk
     const int m = 1 << log_m;
     const unsigned n = (unsigned)(m * L_COLS / 2);
     DevBuf poly, out;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    struct Release {  // the sample buffers and events go on every return path
+        DevBuf &a, &b;
+        cudaEvent_t &x, &y;
+        ~Release() {
+            a.release();
+            b.release();
+            if (x) cudaEventDestroy(x);
+            if (y) cudaEventDestroy(y);
+        }
+    } release{poly, out, e0, e1};
     CKR(poly.reserve((size_t)rows * n * sizeof(fr_t)));
     CKR(out.reserve((size_t)rows * m * sizeof(g1p_t)));
     {  // sample coefficients: a SplitMix64 stream masked below 2^253 < r
@@ -1124,9 +1135,9 @@ int autotune(fk20_ctx *ctx, int log_m, unsigned rows, size_t max_table_bytes, fk
         }
         CK(cudaMemcpy(poly.p, h.data(), h.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
     }
-    Tuner tu{ctx, log_m, rows, st, (const fr_t *)poly.p, (g1p_t *)out.p};
-    CK(cudaEventCreate(&tu.e0));
-    CK(cudaEventCreate(&tu.e1));
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    Tuner tu{ctx, log_m, rows, st, (const fr_t *)poly.p, (g1p_t *)out.p, e0, e1};
     struct Cfg { int window, threads, bps, fused; };
     Cfg best{T->cb, ctx->msm_threads, ctx->fft_blocks_per_sm, ctx->fused_fft};
     float best_ms = 0;
@@ -1176,8 +1187,6 @@ int autotune(fk20_ctx *ctx, int log_m, unsigned rows, size_t max_table_bytes, fk
         if (b != (best.bps ? best.bps : ctx->fused_occupancy)) rc = consider(Cfg{best.window, best.threads, b, 1});
     if (!rc) rc = consider(Cfg{best.window, best.threads, best.bps, best.fused ? 0 : 1});
     apply(best);
-    cudaEventDestroy(tu.e0);
-    cudaEventDestroy(tu.e1);
     cudaStreamSynchronize(st);
     if (rc) return rc;
     res->window = best.window;
@@ -1743,7 +1752,7 @@ extern "C" {
 int fk20_server_create(fk20_server **out, fk20_ctx *ctx, const fk20_server_config *cfg) {
     if (!out || !ctx) return FK20_EINVAL;
     fk20_server_config c = cfg ? *cfg : fk20_server_config{};
-    if (!c.max_rows) c.max_rows = 256;
+    if (!c.max_rows) c.max_rows = 160;
     if (!c.slots) c.slots = 2;
     if (!c.max_queue) c.max_queue = 1u << 16;
     if (c.max_rows > 4096 || c.slots > 8) return FK20_EINVAL;

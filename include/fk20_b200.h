@@ -224,7 +224,7 @@ int fk20_ctx_batch_proofs(fk20_ctx *ctx, uint8_t *proofs, const fr_t *polys, uns
  */
 typedef struct fk20_server fk20_server;
 typedef struct {
-    unsigned max_rows;  /* requests per pack (1..4096; 0 = 256) */
+    unsigned max_rows;  /* requests per pack (1..4096; 0 = 160) */
     unsigned slots;     /* packs in flight at once (1..8; 0 = 2) */
     size_t hbm_budget;  /* device bytes all slots' buffers may hold (0 = half the free memory at creation) */
     unsigned max_queue; /* waiting requests beyond which submit returns FK20_EAGAIN (0 = 1 << 16) */
