@@ -55,7 +55,9 @@ def parse():
                     help="batch: the headline 512 x 4096 batch; serve: Poisson request load through the "
                          "continuous-batching server; ragged: 1000 mixed-length instances as one graph-captured batch; "
                          "micro: kernel microbenchmarks (Fp/Fr products, batched G1 FFT/IFFT, 16-term MSM)")
-    ap.add_argument("--serve-seconds", type=float, default=3.0, help="arrival window per load level (serve)")
+    ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window per load level (serve)")
+    ap.add_argument("--serve-warmup", type=float, default=1.0,
+                    help="seconds of arrivals at the start of each level left out of the statistics (serve)")
     ap.add_argument("--serve-loads", default="0.5,0.9,1.2", help="offered load as fractions of plain-batch capacity")
     ap.add_argument("--serve-max-rows", type=int, default=160)
     ap.add_argument("--serve-slots", type=int, default=2)
@@ -476,7 +478,7 @@ def run_serve(args, ws, rank, dev):
     check = []  # (n, pool index, output) kept for the bit-exactness check
     for frac in [float(x) for x in args.serve_loads.split(",")]:
         rate = frac * plain_pps / mean_proofs  # requests per second
-        count = max(1, int(rate * args.serve_seconds))
+        count = max(1, int(rate * (args.serve_seconds + args.serve_warmup)))
         gaps = rng.exponential(1.0 / rate, count)
         lens = rng.choice(sizes, count, p=weights)
         free = {int(n): [] for n in sizes}
@@ -500,7 +502,11 @@ def run_serve(args, ws, rank, dev):
         srv.reset_stats()
         start = time.perf_counter()
         due = start
+        warm = args.serve_warmup > 0
         for j in range(count):
+            if warm and due - start >= args.serve_warmup:
+                srv.reset_stats()  # steady state: later completions only
+                warm = False
             due += gaps[j]
             d = due - time.perf_counter()
             if d > 0:
@@ -535,7 +541,8 @@ def run_serve(args, ws, rank, dev):
         "config": {"workload": "served load: Poisson arrivals of 1024/2048/4096-coefficient requests "
                                "(weights 0.2/0.3/0.5) at fractions of plain-batch capacity",
                    "window_bits": args.window, "max_rows_per_pack": args.serve_max_rows,
-                   "slots": args.serve_slots, "arrival_window_s": args.serve_seconds, "setup_s": round(setup_s, 2),
+                   "slots": args.serve_slots, "arrival_window_s": args.serve_seconds,
+                   "warmup_s_excluded": args.serve_warmup, "setup_s": round(setup_s, 2),
                    "table_bytes": ctx.device_bytes()},
         "plain_batch": {"rows": rows, "n": n, "proofs_per_s": plain_pps, "latency_ms": plain_ms},
         "loads": loads, "results_same_alone_and_served": same, "checked_requests": len(check),
