@@ -1,10 +1,15 @@
 // engine.cu -- host side of the B200 FK20 engine and its C ABI (include/fk20_b200.h).
 //
 // Owns
-//   - the constant tables (GLV/NAF twiddle programs, Fr twiddles), computed
+//   - the constant tables (GLV/wNAF twiddle programs, Fr twiddles), computed
 //     once on the host from the curve constants and uploaded to every kernel
 //     module of every device used;
-//   - contexts: fixed-base MSM tables per polynomial length, and workspaces;
+//   - contexts: fixed-base MSM tables per polynomial length, commitment
+//     tables, options, a workspace;
+//   - the segment pipeline (run_segments): toeplitz Fr FFTs, one MSM launch
+//     and one persistent G1 FFT launch over up to 8 segments, outputs;
+//   - batch plans (CUDA graphs of that pipeline), the autotuner, and the
+//     continuous-batching request server (a worker thread and its slots);
 //   - the launch sequence of every entry point.
 // There is no CPU compute path: without a usable sm_100 device every entry
 // point returns FK20_ENODEV or the CUDA error.
