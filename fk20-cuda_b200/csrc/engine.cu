@@ -324,6 +324,8 @@ struct fk20_ctx {
     int msm_threads = 128;      // MSM block size (64, 128, 256)
     int fft_blocks_per_sm = 0;  // persistent FFT grid: blocks per SM (0 = as many as fit)
     int fused_occupancy = 1;    // blocks of the persistent FFT kernel that fit on one SM
+    unsigned wait_limit = FUSED_SPIN_LIMIT;  // polls before a persistent wait gives up
+    unsigned unpublished = 0xffffffffu;      // test hook: a task whose completion is not published
     std::mutex mu;
     Tables tab[3];  // log_m 7, 8, 9
     struct {        // KZG commitment tables over setup points s_0 .. s_{n-1}
@@ -603,6 +605,8 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
         p.next = (unsigned *)ws.sync.p;
         p.err = (int *)((char *)ws.sync.p + 128);
         p.epoch = 1;  // counters are cleared before every launch
+        p.spin_limit = ctx->wait_limit;
+        p.unpublished = ctx->unpublished;
         // persistent grid: the context's setting, or the caller's share of the SMs (server packs)
         int per_sm = ctx->fused_occupancy;
         const int want = fft_bps > 0 ? fft_bps : ctx->fft_blocks_per_sm;
@@ -809,6 +813,13 @@ int fk20_ctx_set(fk20_ctx *ctx, int option, int value) {
         if (value < 0 || value > 64) return FK20_EINVAL;
         ctx->fft_blocks_per_sm = value;
         return 0;
+    case FK20_OPT_WAIT_LIMIT:
+        if (value < 0) return FK20_EINVAL;
+        ctx->wait_limit = value ? (unsigned)value : FUSED_SPIN_LIMIT;
+        return 0;
+    case FK20_OPT_TEST_UNPUBLISHED_TASK:
+        ctx->unpublished = value < 0 ? 0xffffffffu : (unsigned)value;
+        return 0;
     default: return FK20_EINVAL;
     }
 }
@@ -971,6 +982,8 @@ int fk20_ctx_get(fk20_ctx *ctx, int option, int *value) {
     case FK20_OPT_FUSED_FFT: *value = ctx->fused_fft; return 0;
     case FK20_OPT_MSM_THREADS: *value = ctx->msm_threads; return 0;
     case FK20_OPT_FFT_BLOCKS_PER_SM: *value = ctx->fft_blocks_per_sm; return 0;
+    case FK20_OPT_WAIT_LIMIT: *value = (int)ctx->wait_limit; return 0;
+    case FK20_OPT_TEST_UNPUBLISHED_TASK: *value = ctx->unpublished == 0xffffffffu ? -1 : (int)ctx->unpublished; return 0;
     default: return FK20_EINVAL;
     }
 }

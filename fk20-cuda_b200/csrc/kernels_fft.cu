@@ -103,10 +103,9 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__
 // the task's stores).  Tasks go only to running warps and a task only waits on
 // tasks of lower index, so the lowest unfinished task never waits and every
 // wait ends, also when not all blocks are resident.  The wait is still bounded
-// (FUSED_SPIN_LIMIT polls): on expiry the kernel records an error code and
+// (plan.spin_limit polls, default FUSED_SPIN_LIMIT): on expiry the kernel records an error code and
 // returns instead of hanging.  Tile data written by other SMs is read through
 // L2 (ld.cg) so no stale L1 line is used.
-constexpr unsigned FUSED_SPIN_LIMIT = 1u << 24;
 
 FK_D void tile_to_slot_cg(const StridedPoint &slot, const uint4 *base, int lane) {
 #pragma unroll
@@ -138,12 +137,12 @@ FK_D void st_release(unsigned *p, unsigned v) {
 }
 
 // lane 0 waits until ready[a] and ready[b] reach `need`; false on timeout
-FK_D bool wait_ready(const unsigned *ra, const unsigned *rb, unsigned need, int lane) {
+FK_D bool wait_ready(const unsigned *ra, const unsigned *rb, unsigned need, int lane, unsigned limit) {
     int ok = 1;
     if (lane == 0) {
         unsigned spins = 0;
         while (ld_acquire(ra) < need || ld_acquire(rb) < need) {
-            if (++spins >= FUSED_SPIN_LIMIT) { ok = 0; break; }
+            if (++spins >= limit) { ok = 0; break; }
             __nanosleep(64);
         }
     }
@@ -171,7 +170,7 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_fused(const __g
         const int m = 1 << P.blk.log_m[t.seg];
         const int S = t.S, g = t.g, i0 = t.i0, i1 = t.i1, tix = t.tix, kind = t.kind;
         unsigned *r0 = a.ready + (size_t)g * m + i0, *r1 = a.ready + (size_t)g * m + i1;
-        if (S > 0 && !wait_ready(r0, r1, base + (unsigned)S, lane)) {
+        if (S > 0 && !wait_ready(r0, r1, base + (unsigned)S, lane, P.spin_limit)) {
             if (lane == 0) atomicCAS(P.err, 0, 1000 + S);
             return;
         }
@@ -215,8 +214,10 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_fused(const __g
         __threadfence();
         __syncwarp();
         if (lane == 0) {
-            st_release(r0, base + (unsigned)S + 1u);
-            st_release(r1, base + (unsigned)S + 1u);
+            if (task != P.unpublished) {  // see FusedPlan::unpublished (tests of the bounded wait)
+                st_release(r0, base + (unsigned)S + 1u);
+                st_release(r1, base + (unsigned)S + 1u);
+            }
         }
     }
 }

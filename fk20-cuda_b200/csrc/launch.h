@@ -41,7 +41,13 @@ struct FusedPlan {
     int *err;        // 0 = ok, else 1000 + stage that timed out
     unsigned epoch;  // readiness value base (epoch * 64 + stage + 1), < 2^26
     int blocks;      // grid size: resident blocks of the persistent launch
+    unsigned spin_limit;   // polls before a readiness wait gives up
+    // A task whose completion is not published (0xffffffff: none).  Set only
+    // by tests of the bounded wait: the tasks that read its positions wait
+    // until spin_limit, and the launch ends with the error flag set.
+    unsigned unpublished;
 };
+constexpr unsigned FUSED_SPIN_LIMIT = 1u << 24;  // default spin_limit
 
 // per-module constant upload (one per translation unit)
 cudaError_t upload_consts_fr();

@@ -51,6 +51,8 @@ FK20_EAGAIN = 1007
 FK20_OPT_FUSED_FFT = 1
 FK20_OPT_MSM_THREADS = 2
 FK20_OPT_FFT_BLOCKS_PER_SM = 3
+FK20_OPT_WAIT_LIMIT = 4
+FK20_OPT_TEST_UNPUBLISHED_TASK = 5
 
 
 class TuneResult(ctypes.Structure):

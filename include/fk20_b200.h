@@ -138,6 +138,15 @@ int fk20_ctx_autotune(fk20_ctx *ctx, unsigned n, unsigned rows, size_t max_table
 /* FK20_OPT_FFT_BLOCKS_PER_SM: persistent FFT grid, blocks per SM (0 =
  * default: as many as fit). */
 #define FK20_OPT_FFT_BLOCKS_PER_SM 3
+/* FK20_OPT_WAIT_LIMIT: polls a readiness wait of the persistent FFT makes
+ * before it gives up and the launch reports FK20_ETIMEOUT (0 = default 2^24). */
+#define FK20_OPT_WAIT_LIMIT 4
+/* FK20_OPT_TEST_UNPUBLISHED_TASK: for tests of that bounded wait only -- the
+ * task of this index in the next persistent launches never publishes its
+ * completion, so the tasks that read its outputs wait until the limit and
+ * the call's results are invalid (fk20_ctx_status returns FK20_ETIMEOUT and
+ * clears the condition).  -1 (default) = off. */
+#define FK20_OPT_TEST_UNPUBLISHED_TASK 5
 int fk20_ctx_set(fk20_ctx *ctx, int option, int value);
 int fk20_ctx_get(fk20_ctx *ctx, int option, int *value);
 

@@ -377,3 +377,31 @@ def test_row_counts_around_group_boundaries(engine, rows):
     for r, j in [(0, 3), (rows - 1, 509), (rows // 2, 256)]:
         direct = O.kzg_direct(poly[r], tau, 16, j, j + 1)[0]
         assert np.array_equal(O.g1_normalize(got[r, j]), direct), (rows, r, j)
+
+
+def test_bounded_wait_reports_timeout_and_context_recovers(engine):
+    """The persistent FFT's readiness waits are bounded: with a short limit and
+    one task that never publishes its completion (a flag nothing sets), the
+    tasks that read its outputs give up, the call reports FK20_ETIMEOUT through
+    fk20_ctx_status, and the context works normally afterwards."""
+    import torch
+    n, rows, m = 1024, 40, 128
+    c = engine.Context(0, 8)
+    c.load_xext_fft(n, engine.to_device(fk20_setup_data(n)[2]))
+    poly = engine.to_device(O.seeded_fr(8800, rows * n).reshape(rows, n, 4))
+    good = engine.empty((rows, m, 18))
+    c.poly2h_fft(good, poly, rows, n)
+    assert c.status() == 0
+    c.set(engine.FK20_OPT_WAIT_LIMIT, 1 << 12)
+    c.set(engine.FK20_OPT_TEST_UNPUBLISHED_TASK, 5)  # a first-stage butterfly of row group 1
+    bad = engine.empty((rows, m, 18))
+    c.poly2h_fft(bad, poly, rows, n)
+    assert c.status() == engine.FK20_ETIMEOUT
+    c.set(engine.FK20_OPT_TEST_UNPUBLISHED_TASK, -1)
+    c.set(engine.FK20_OPT_WAIT_LIMIT, 0)
+    again = engine.empty((rows, m, 18))
+    c.poly2h_fft(again, poly, rows, n)
+    assert c.status() == 0
+    torch.cuda.synchronize()
+    assert torch.equal(again, good)
+    c.close()
