@@ -61,7 +61,9 @@ def parse():
     ap.add_argument("--serve-loads", default="0.5,0.9,1.2", help="offered load as fractions of plain-batch capacity")
     ap.add_argument("--serve-max-rows", type=int, default=160)
     ap.add_argument("--serve-slots", type=int, default=2)
-    ap.add_argument("--autotune", action="store_true", help="ragged: autotune the context first")
+    ap.add_argument("--autotune", action="store_true", help="autotune the context before timing (batch, ragged)")
+    ap.add_argument("--tune-max-table-bytes", type=int, default=0,
+                    help="table memory budget of the autotuner (0 = what the free device memory allows)")
     return ap.parse_args()
 
 
@@ -304,6 +306,11 @@ def run_ours(args, ws, rank, dev):
     ctx.load_setup(n, setup)
     torch.cuda.synchronize()
     setup_s = time.time() - t0
+    tune = None
+    if args.autotune:  # window within the memory budget, MSM block size, FFT grid, fused vs staged
+        t1 = time.time()
+        tune = ctx.autotune(n, rows=min(rows, 512), max_table_bytes=args.tune_max_table_bytes)
+        tune["tune_s"] = round(time.time() - t1, 1)
 
     poly_h = seeded_polys(rank_rows_seed(rank), rows, n)
     poly = E.to_device(poly_h)
@@ -420,7 +427,7 @@ def run_ours(args, ws, rank, dev):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded uniform Fr, seeded tau)",
         "config": workload_config(args, {"setup_s": round(setup_s, 2),
-                                         "table_bytes": ctx.device_bytes()}),
+                                         "table_bytes": ctx.device_bytes(), "autotune": tune}),
         "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "impl": "ours",
     }
