@@ -18,8 +18,12 @@
 #ifndef FK_MSM_MINB
 #define FK_MSM_MINB 1
 #endif
-// block sizes the launcher accepts: 64, 128 (default) or 256 threads
-constexpr int MSM_MAX_THREADS = 256;
+// largest block size the launcher may use (64, 128 or 256 threads; the
+// launch bounds cap registers at 65536 / (FK_MSM_MAX_THREADS * FK_MSM_MINB))
+#ifndef FK_MSM_MAX_THREADS
+#define FK_MSM_MAX_THREADS 256
+#endif
+constexpr int MSM_MAX_THREADS = FK_MSM_MAX_THREADS;
 
 namespace fk {
 
@@ -153,6 +157,7 @@ void launch_commit(uint64_t *out, uint4 *part, const uint64_t *poly, const uint4
 
 void launch_msm(const MsmArgs &a, int threads, cudaStream_t st) {
     if (threads != 64 && threads != 128 && threads != 256) threads = 128;
+    if (threads > MSM_MAX_THREADS) threads = MSM_MAX_THREADS;
     k_msm<<<blocks_for(a.warps, (unsigned)threads / 32), threads, 0, st>>>(a);
 }
 
