@@ -134,8 +134,8 @@ class ClockSampler:
     def __init__(self, dev: int):
         self.dev = dev
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 f".clocks_{os.getpid()}.csv")
+        import tempfile
+        self.path = os.path.join(tempfile.gettempdir(), f"fk20_clocks_{os.getpid()}_{dev}.csv")
 
     def __enter__(self):
         try:
