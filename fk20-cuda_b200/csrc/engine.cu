@@ -1430,6 +1430,36 @@ int fr_fft_n(fr_t *output, const fr_t *input, unsigned log_m, unsigned count, in
 int fr_fft(fr_t *output, const fr_t *input, unsigned count, void *stream) { return fr_fft_n(output, input, 9, count, 0, stream); }
 int fr_ift(fr_t *output, const fr_t *input, unsigned count, void *stream) { return fr_fft_n(output, input, 9, count, 1, stream); }
 
+// ---------------------------------------------------------------- pairings
+int fk20_pairing_check_n(uint8_t *ok, const g1p_t *a, const g2p_t *b, const g1p_t *c, const g2p_t *d, size_t count,
+                         void *stream) {
+    if (!ok || !a || !b || !c || !d || count == 0) return FK20_EINVAL;
+    CKR(current_device_ready());
+    launch_pairing(1, nullptr, ok, (const uint64_t *)a, (const uint64_t *)b, (const uint64_t *)c,
+                   (const uint64_t *)d, count, S_(stream));
+    CKL();
+    return 0;
+}
+
+int fk20_pairing_n(fp_t *out, const g1p_t *a, const g2p_t *b, size_t count, void *stream) {
+    if (!out || !a || !b || count == 0) return FK20_EINVAL;
+    CKR(current_device_ready());
+    launch_pairing(0, (uint64_t *)out, nullptr, (const uint64_t *)a, (const uint64_t *)b, nullptr, nullptr, count,
+                   S_(stream));
+    CKL();
+    return 0;
+}
+
+int g2p_op_n(int op, g2p_t *out, const g2p_t *a, const void *b, size_t count, void *stream) {
+    if (!a || op < 0 || op > 6 || count == 0) return FK20_EINVAL;
+    if (op != 6 && !out) return FK20_EINVAL;
+    if ((op == 0 || op == 3 || op == 4 || op == 6) && !b) return FK20_EINVAL;
+    CKR(current_device_ready());
+    launch_g2_op(op, (uint64_t *)out, (const uint64_t *)a, b, count, S_(stream));
+    CKL();
+    return 0;
+}
+
 // ---------------------------------------------------------------- element-wise
 int fp_op_n(int op, fp_t *out, const fp_t *a, const fp_t *b, size_t count, void *stream) {
     if (!out || !a || op < 0 || op > 11 || count == 0) return FK20_EINVAL;

@@ -89,6 +89,11 @@ void launch_h_fft_to_proofs(uint8_t *out, const uint64_t *h, int rows, int log_m
 void launch_tile_to_proofs(uint8_t *out, const uint4 *D, const size_t *out_off, int rows, int log_m,
                            cudaStream_t st);
 
+// kernels_pairing.cu: op 0 pairing values, op 1 pairing checks; G2 element-wise ops
+void launch_pairing(int op, uint64_t *out, uint8_t *ok, const uint64_t *a, const uint64_t *b, const uint64_t *c,
+                    const uint64_t *d, size_t count, cudaStream_t st);
+void launch_g2_op(int op, uint64_t *out, const uint64_t *a, const void *b, size_t count, cudaStream_t st);
+
 // kernels_tables.cu
 size_t table_window_base_bytes();  // sizeof(G1P)
 size_t table_z_bytes();            // sizeof(Fp)

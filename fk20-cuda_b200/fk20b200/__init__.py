@@ -25,6 +25,7 @@ FK20_ENODEV = 1004
 FIELD_OPS = {"mul": 0, "sqr": 1, "add": 2, "sub": 3, "neg": 4, "inv": 5, "reduce": 6,
              "x2": 7, "x3": 8, "x4": 9, "x8": 10, "x12": 11}
 G1_OPS = {"add": 0, "dbl": 1, "neg": 2, "sub": 3, "mul": 4, "normalize": 5, "is_point": 6}
+G2_OPS = {"add": 0, "dbl": 1, "neg": 2, "sub": 3, "mul": 4, "normalize": 5, "is_point": 6}
 
 # every symbol declared in include/fk20_b200.h
 ABI_SYMBOLS = (
@@ -40,7 +41,7 @@ ABI_SYMBOLS = (
     "fk20_plan_launch", "fk20_plan_destroy", "fk20_ctx_autotune", "fk20_server_create", "fk20_server_submit",
     "fk20_server_wait", "fk20_server_get_stats", "fk20_server_reset_stats", "fk20_server_destroy",
     "fk20_g1p_compress_n", "fk20_h_fft2proofs", "fk20_ctx_poly2proofs", "fk20_ctx_batch_proofs",
-    "fk20_ctx_load_commit", "fk20_ctx_commit",
+    "fk20_ctx_load_commit", "fk20_ctx_commit", "fk20_pairing_check_n", "fk20_pairing_n", "g2p_op_n",
 )
 
 # kernel kinds of the per-launch profiler (FK20_K_* in the header)
@@ -156,6 +157,9 @@ def lib() -> ctypes.CDLL:
             "fk20_ctx_batch_proofs": ([vp, vp, vp, u, vp, vp, vp, vp], i),
             "fk20_ctx_load_commit": ([vp, u, vp, i, vp], i),
             "fk20_ctx_commit": ([vp, vp, vp, u, u, vp], i),
+            "fk20_pairing_check_n": ([vp, vp, vp, vp, vp, sz, vp], i),
+            "fk20_pairing_n": ([vp, vp, vp, sz, vp], i),
+            "g2p_op_n": ([i, vp, vp, vp, sz, vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

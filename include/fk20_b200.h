@@ -215,6 +215,28 @@ int fk20_ctx_poly2proofs(fk20_ctx *ctx, uint8_t *proofs, const fr_t *polynomial,
 int fk20_ctx_batch_proofs(fk20_ctx *ctx, uint8_t *proofs, const fr_t *polys, unsigned count, const unsigned *n,
                           const size_t *poly_off, const size_t *out_off, void *stream);
 
+/* ------------------------------------------------------------------ pairings (proof verification)
+ * BLS12-381 pairing checks for verifying KZG proofs: the reference's
+ * check_proof_multi (FK20Py/kzg_proofs.py:207-232) pairs with py_ecc and has no
+ * CUDA counterpart.  G2 points are on the twist y^2 = x^3 + 4(1 + u) over
+ * Fp2 = Fp[u]/(u^2 + 1), an Fp2 element being {c0, c1} = c0 + c1 u; g2p_t is
+ * homogeneous projective in standard form, infinity written as (0, 1, 0).
+ * The pairing is the optimal ate pairing of BLS12 curves (up to a fixed
+ * exponent: non-degenerate and bilinear, which is what the checks use).  One
+ * thread per check; a launch takes about 1.2 s whatever its count up to ~10^4
+ * checks (B200): for verification, not proving. */
+typedef struct { fp_t x[2], y[2], z[2]; } g2p_t;
+
+/* ok[i] = (e(a[i], b[i]) == e(c[i], d[i])); a KZG multiproof check is
+ * e(C - [I(s)]G1, G2) == e(proof, [s^l - x^l]G2). */
+int fk20_pairing_check_n(uint8_t *ok, const g1p_t *a, const g2p_t *b, const g1p_t *c, const g2p_t *d, size_t count,
+                         void *stream);
+/* out[i][12] = e(a[i], b[i]) as the 6 Fp2 coefficients of w in Fp12 = Fp2[w]/(w^6 - (1 + u)) */
+int fk20_pairing_n(fp_t *out, const g1p_t *a, const g2p_t *b, size_t count, void *stream);
+/* G2 element-wise: 0 add, 1 dbl, 2 neg, 3 sub, 4 mul by fr_t scalar (b), 5 normalise,
+ * 6 on-curve flag (b: uint8 out). */
+int g2p_op_n(int op, g2p_t *out, const g2p_t *a, const void *b, size_t count, void *stream);
+
 /* ------------------------------------------------------------------ request server
  * Continuous batching of blob-proof requests (no reference counterpart: the
  * reference has no serving layer).  A worker thread admits requests as they

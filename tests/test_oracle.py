@@ -224,3 +224,23 @@ def test_reverse_bit_order_matches_reference_definition():
         j = int(('{:0' + str(m.bit_length() - 1) + 'b}').format(i)[::-1], 2)
         assert np.array_equal(r[:, i], rows[:, j])
     assert np.array_equal(O.reverse_bit_order(r), rows)
+
+
+def test_pairing_restatement_is_bilinear():
+    """The pairing checker (oracle/pairing_py.py): non-degenerate, bilinear,
+    and the verification equation holds exactly for matching exponents."""
+    import pairing_py as PP
+    g = O.g1_generator()
+
+    def g1mul(k):
+        p = O.g1_op("mul", g.reshape(1, 18), O.int_to_limbs(k % O.R, 4).reshape(1, 4))[0]
+        return (O.limbs_to_int(p[0:6]), O.limbs_to_int(p[6:12]))
+
+    G1, G2 = g1mul(1), PP.g2_generator()
+    assert PP.g2mul(O.R, G2) is None  # the generator has order r
+    e = PP.pairing(G1, G2)
+    assert e != PP.ONE12 and PP.f12pow(e, O.R) == PP.ONE12
+    a, b = 0x1234567890ABCDEF, 0xFEDCBA0987654321
+    assert PP.pairing(g1mul(a), PP.g2mul(b, G2)) == PP.f12pow(e, a * b % O.R)
+    assert PP.pairing_check(g1mul(a), PP.g2mul(b, G2), g1mul(a * b), G2)
+    assert not PP.pairing_check(g1mul(a), PP.g2mul(b, G2), g1mul(a * b + 1), G2)
