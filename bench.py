@@ -55,12 +55,16 @@ def parse():
                     help="batch: the headline 512 x 4096 batch; serve: Poisson request load through the "
                          "continuous-batching server; ragged: 1000 mixed-length instances as one graph-captured batch; "
                          "micro: kernel microbenchmarks (Fp/Fr products, batched G1 FFT/IFFT, 16-term MSM)")
-    ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window per load level (serve)")
+    ap.add_argument("--serve-seconds", type=float, default=8.0, help="arrival window per load level (serve)")
     ap.add_argument("--serve-warmup", type=float, default=1.0,
                     help="seconds of arrivals at the start of each level left out of the statistics (serve)")
-    ap.add_argument("--serve-loads", default="0.5,0.9,1.2", help="offered load as fractions of plain-batch capacity")
+    ap.add_argument("--serve-loads", default="0.5,0.8,0.9,1.2", help="offered load as fractions of plain-batch capacity")
     ap.add_argument("--serve-max-rows", type=int, default=160)
     ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--serve-fft-blocks", type=int, default=0,
+                    help="persistent-FFT blocks per SM of each pack (0: adaptive to the backlog)")
+    ap.add_argument("--serve-latency-rows", type=int, default=0,
+                    help="latency-mode packs while at most this many requests wait (0: max rows)")
     ap.add_argument("--autotune", action="store_true", help="autotune the context before timing (batch, ragged)")
     ap.add_argument("--tune-max-table-bytes", type=int, default=0,
                     help="table memory budget of the autotuner (0 = what the free device memory allows)")
@@ -479,7 +483,8 @@ def run_serve(args, ws, rank, dev):
     sizes = np.array([n for n, _ in SERVE_MIX])
     weights = np.array([w for _, w in SERVE_MIX])
     mean_proofs = float((sizes // 8 * weights).sum())
-    srv = E.Server(ctx, max_rows=args.serve_max_rows, slots=args.serve_slots)
+    srv = E.Server(ctx, max_rows=args.serve_max_rows, slots=args.serve_slots, fft_blocks_per_sm=args.serve_fft_blocks,
+                   latency_rows=args.serve_latency_rows)
     loads = []
     rng = np.random.default_rng(42)
     check = []  # (n, pool index, output) kept for the bit-exactness check
@@ -548,11 +553,16 @@ def run_serve(args, ws, rank, dev):
         "config": {"workload": "served load: Poisson arrivals of 1024/2048/4096-coefficient requests "
                                "(weights 0.2/0.3/0.5) at fractions of plain-batch capacity",
                    "window_bits": args.window, "max_rows_per_pack": args.serve_max_rows,
-                   "slots": args.serve_slots, "arrival_window_s": args.serve_seconds,
+                   "slots": args.serve_slots, "fft_blocks_per_sm": args.serve_fft_blocks or "adaptive",
+                   "latency_rows": args.serve_latency_rows or args.serve_max_rows, "arrival_window_s": args.serve_seconds,
                    "warmup_s_excluded": args.serve_warmup, "setup_s": round(setup_s, 2),
                    "table_bytes": ctx.device_bytes()},
         "plain_batch": {"rows": rows, "n": n, "proofs_per_s": plain_pps, "latency_ms": plain_ms},
-        "loads": loads, "results_same_alone_and_served": same, "checked_requests": len(check),
+        "loads": loads,
+        # load levels that serve >= 80 % of plain-batch proofs/s with p99 below the plain batch's latency
+        "loads_at_80pct_with_p99_below_plain": [x["load"] for x in loads
+                                                 if x["served_vs_plain"] >= 0.8 and x["p99_below_plain_batch_latency"]],
+        "results_same_alone_and_served": same, "checked_requests": len(check),
         "impl": "ours",
     }
     ctx.close()

@@ -1622,7 +1622,7 @@ void CUDART_CB pack_done_cb(void *p) {
 }
 
 // inputs to pinned staging, one H2D copy, the segment pipeline, one D2H copy
-int enqueue_pack(fk20_server *s, Slot &sl) {
+int enqueue_pack(fk20_server *s, Slot &sl, bool latency) {
     const size_t cnt = sl.reqs.size();
     std::vector<unsigned> ns(cnt);
     std::vector<size_t> poly_off(cnt), out_off(cnt);
@@ -1648,9 +1648,17 @@ int enqueue_pack(fk20_server *s, Slot &sl) {
         Seg sg[3];
         int nseg = 0;
         CKR(batch_segments(ctx, sl.ws, (unsigned)cnt, ns.data(), poly_off.data(), out_off.data(), sg, &nseg, sl.st));
-        // each pack's persistent FFT takes a share of the SMs, so packs of
-        // different slots run side by side instead of one after the other
-        const int share = std::max(1, ctx->fused_occupancy / (int)s->slots.size());
+        // The persistent FFT's blocks per SM.  Adaptive by default: a
+        // latency-mode pack may fill the GPU, and the next pack's blocks take
+        // over as its own retire (a pack alone finishes in about half the
+        // time); a throughput-mode pack takes 1/slots of the SMs, so packs of
+        // different slots run side by side and hide each other's dependency
+        // waits.
+        int share = ctx->fused_occupancy;
+        if (s->cfg.fft_blocks_per_sm)
+            share = std::min((int)s->cfg.fft_blocks_per_sm, ctx->fused_occupancy);
+        else if (!latency)
+            share = std::max(1, ctx->fused_occupancy / (int)s->slots.size());
         CKR(run_segments(ctx, sl.ws, sg, nseg, (const fr_t *)sl.dpoly.p, (g1p_t *)sl.dout.p, true, sl.st, false,
                          share));
     }
@@ -1708,11 +1716,14 @@ void server_main(fk20_server *s) {
             else others += sl.bytes();
         }
         if (fs && !s->queue.empty()) {
-            // Oldest first, up to max_rows and the memory budget.  When more
-            // requests wait than a pack takes, each length with 32 or more in
-            // the pack keeps a multiple of 32 (a warp proves 32 rows of one
+            // Latency mode while no more than latency_rows requests wait: the
+            // pack takes them all.  Beyond that (a burst, or a load above what
+            // latency-mode packs sustain), throughput mode: oldest first, up to
+            // max_rows and the memory budget, and each length with 32 or more
+            // in the pack keeps a multiple of 32 (a warp proves 32 rows of one
             // length; a partial group idles lanes): its youngest extra
             // requests go back to the head of the queue for the next pack.
+            const bool latency = s->queue.size() <= s->cfg.latency_rows;
             const bool more = s->queue.size() > s->cfg.max_rows;
             unsigned cnt[3] = {0, 0, 0};
             size_t q = 0;
@@ -1758,7 +1769,7 @@ void server_main(fk20_server *s) {
                 continue;
             } else {
                 lk.unlock();
-                fs->rc = enqueue_pack(s, *fs);
+                fs->rc = enqueue_pack(s, *fs, latency);
                 lk.lock();
                 continue;
             }
@@ -1801,6 +1812,8 @@ int fk20_server_create(fk20_server **out, fk20_ctx *ctx, const fk20_server_confi
     if (!out || !ctx) return FK20_EINVAL;
     fk20_server_config c = cfg ? *cfg : fk20_server_config{};
     if (!c.max_rows) c.max_rows = 160;
+    if (!c.latency_rows) c.latency_rows = c.max_rows;
+    if (c.latency_rows > c.max_rows) return FK20_EINVAL;
     if (!c.slots) c.slots = 2;
     if (!c.max_queue) c.max_queue = 1u << 16;
     if (c.max_rows > 4096 || c.slots > 8) return FK20_EINVAL;

@@ -63,7 +63,8 @@ class TuneResult(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("max_rows", ctypes.c_uint), ("slots", ctypes.c_uint), ("hbm_budget", ctypes.c_size_t),
-                ("max_queue", ctypes.c_uint)]
+                ("max_queue", ctypes.c_uint), ("fft_blocks_per_sm", ctypes.c_uint),
+                ("latency_rows", ctypes.c_uint)]
 
 
 class ServerStats(ctypes.Structure):
@@ -342,8 +343,9 @@ class Server:
     submit() takes HOST numpy arrays: the polynomial (n x 4 uint64) and the
     output (n/8 x 18 uint64); both are kept referenced until wait()."""
 
-    def __init__(self, ctx: Context, max_rows: int = 128, slots: int = 2, hbm_budget: int = 0, max_queue: int = 0):
-        cfg = ServerConfig(max_rows, slots, hbm_budget, max_queue)
+    def __init__(self, ctx: Context, max_rows: int = 0, slots: int = 0, hbm_budget: int = 0, max_queue: int = 0,
+                 fft_blocks_per_sm: int = 0, latency_rows: int = 0):
+        cfg = ServerConfig(max_rows, slots, hbm_budget, max_queue, fft_blocks_per_sm, latency_rows)
         h = ctypes.c_void_p()
         call("fk20_server_create", ctypes.byref(h), ctx.h, ctypes.byref(cfg))
         self.h = h

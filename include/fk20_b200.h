@@ -242,12 +242,13 @@ int g2p_op_n(int op, g2p_t *out, const g2p_t *a, const void *b, size_t count, vo
  * reference has no serving layer).  A worker thread admits requests as they
  * arrive: whenever one of `slots` slots (a stream, a workspace, device and
  * pinned staging buffers) is free, it packs the waiting requests -- mixed
- * lengths, oldest first, whole groups of 32 rows per length when more are
- * waiting than a pack takes -- up to max_rows and the device-memory budget,
- * and enqueues them as one segment pipeline (one MSM launch and one
- * persistent G1 FFT launch over all lengths).  Packs of different slots
- * run side by side on the device (each pack's persistent FFT takes a share
- * of the SMs); requests that arrive meanwhile wait for the next free slot.
+ * lengths, oldest first, up to max_rows and the device-memory budget -- and
+ * enqueues them as one segment pipeline (one MSM launch and one persistent
+ * G1 FFT launch over all lengths).  While few requests wait (latency mode)
+ * a pack takes them all and its FFT may fill the GPU; when more wait
+ * (throughput mode) a pack keeps whole groups of 32 rows per length and
+ * packs of different slots split the SMs and run side by side.  Requests
+ * that arrive meanwhile wait for the next free slot.
  * Slot buffers are sized for a full pack at creation when that fits the
  * budget.  The setup tables stay resident in the context (load every
  * length the requests use first).  Each request's result is the same as a
@@ -259,6 +260,13 @@ typedef struct {
     unsigned slots;     /* packs in flight at once (1..8; 0 = 2) */
     size_t hbm_budget;  /* device bytes all slots' buffers may hold (0 = half the free memory at creation) */
     unsigned max_queue; /* waiting requests beyond which submit returns FK20_EAGAIN (0 = 1 << 16) */
+    unsigned fft_blocks_per_sm; /* persistent-FFT blocks per SM of each pack.  0 = adaptive: the kernel's
+                                   occupancy in latency mode (a pack may fill the GPU, and the next one's blocks
+                                   take over as its blocks retire), occupancy / slots in throughput mode (packs
+                                   split the SMs and run side by side) */
+    unsigned latency_rows;      /* latency mode while at most this many requests wait: a pack takes them all;
+                                   beyond it, throughput mode: packs of up to max_rows, whole 32-row groups per
+                                   length (0 = max_rows; <= max_rows) */
 } fk20_server_config;
 typedef struct {
     uint64_t requests, proofs, packs;

@@ -21,13 +21,17 @@ def served_ctx(engine):
     c.close()
 
 
-def test_server_results_same_alone_and_in_the_mix(engine, served_ctx):
-    import torch
+@pytest.mark.parametrize("mode", [{}, {"latency_rows": 4}, {"fft_blocks_per_sm": 1}],
+                         ids=["adaptive", "latency-rows-4", "one-fft-block-per-sm"])
+def test_server_results_same_alone_and_in_the_mix(engine, served_ctx, mode):
+    """Latency-mode packs (the whole queue, the whole GPU) and throughput-mode
+    packs (whole 32-row groups, the SMs split between slots) both occur here:
+    bursts of 10 submissions against 16-request packs."""
     rng = np.random.default_rng(5)
     sizes = [int(x) for x in rng.choice([1024, 2048, 4096], 90, p=[0.2, 0.3, 0.5])]
     polys = [O.seeded_fr(4000 + j, n) for j, n in enumerate(sizes)]
     outs = [np.zeros((n // 8, 18), np.uint64) for n in sizes]
-    srv = engine.Server(served_ctx, max_rows=16, slots=2)
+    srv = engine.Server(served_ctx, max_rows=16, slots=2, **mode)
     tickets = []
     for j, n in enumerate(sizes):  # arrivals spread over time, so packs overlap with new arrivals
         tickets.append(srv.submit(polys[j], outs[j]))
@@ -56,6 +60,9 @@ def test_server_rejects_bad_requests(engine, served_ctx):
     bad = np.zeros((3000, 4), np.uint64)
     with pytest.raises(engine.Fk20Error) as e:
         srv.submit(bad, np.zeros((375, 18), np.uint64))
+    assert e.value.code == engine.FK20_EINVAL
+    with pytest.raises(engine.Fk20Error) as e:
+        engine.Server(served_ctx, max_rows=8, latency_rows=9)  # latency_rows above max_rows
     assert e.value.code == engine.FK20_EINVAL
     assert srv.wait(12345, 0) == engine.FK20_EINVAL
     p = O.seeded_fr(1, 1024)
