@@ -2,21 +2,33 @@
 //
 // The reference verifies multiproofs with py_ecc's pairing (check_proof_multi,
 // FK20Py/kzg_proofs.py:207-232; no CUDA counterpart).  This is the optimal
-// ate pairing of BLS12 curves in its plainest form -- verification is not on
-// the proving hot path:
-//   * Fp2 = Fp[u]/(u^2 + 1); Fp12 = Fp2[w]/(w^6 - xi), xi = 1 + u, an element
-//     kept as its 6 coefficients of w.
+// ate pairing of BLS12 curves computed with the standard techniques:
+//   * Fp2 = Fp[u]/(u^2 + 1), Fp6 = Fp2[v]/(v^3 - xi), Fp12 = Fp6[w]/(w^2 - v),
+//     xi = 1 + u (so w^6 = xi); Karatsuba products at every level (an Fp12
+//     product is 18 Fp2 products, a square 12).
 //   * G2 on the M-type twist E': y^2 = x^3 + 4 xi, mapped into E(Fp12) by
 //     psi(x', y') = (x'/w^2, y'/w^3).
-//   * Miller loop over the bits of |z| = 0xd201000000010000, T affine; the
-//     line through T with twist slope L evaluated at P, scaled by w^3:
-//     (L xT - yT) + (-L xP) w^2 + yP w^3 (w^3 and the vertical lines vanish
-//     in the final exponentiation).  As z < 0 and the loop runs over |z|, the
-//     value is the usual pairing's inverse: still non-degenerate and bilinear.
-//   * Final exponentiation by (p^12 - 1)/r as one exponent
-//     (pairing_consts.inc, generated by gen_pairing_consts.py).
-// One thread per pairing or check; Fp12 values live in local memory and the
-// Fp2 / Fp12 products are out-of-line routines, which keeps the code small.
+//   * Miller loop over the bits of |z| = 0xd201000000010000 with T in
+//     homogeneous projective coordinates (no inversions); the line through T
+//     (tangent, or chord through Q) evaluated at P is c0 + c2 w^2 + c3 w^3
+//     up to a factor in Fp2, which the final exponentiation removes:
+//       tangent: c0 = Y^2 - 3b'Z^2, c2 = -3X^2 xP, c3 = 2YZ yP;
+//       chord:   c0 = th xQ - la yQ, c2 = -th xP, c3 = la yP,
+//                th = Y - yQ Z, la = X - xQ Z.
+//     Both pairings of a check share one loop (one squaring of f per bit).
+//     As z < 0 and the loop runs over |z|, the value is the inverse of the
+//     usual normalisation: non-degenerate and bilinear all the same.
+//   * Final exponentiation by 3 (p^12 - 1)/r: the easy part
+//     m = f^((p^6 - 1)(p^2 + 1)) by conjugation, one inversion and a
+//     Frobenius map; the hard part by the decomposition
+//     3 (p^4 - p^2 + 1)/r = (z - 1)^2 (z + p)(z^2 + p^2 - 1) + 3
+//     (five exponentiations by z, Frobenius maps, conjugations for the
+//     inverses of the cyclotomic subgroup).  A fixed exponent coprime to r
+//     keeps a check's answer the same: f^(3(p^12-1)/r) == 1 exactly when
+//     f^((p^12-1)/r) == 1.
+// One thread per pairing or check; field elements live in local memory and
+// the Fp2 / Fp6 / Fp12 products are out-of-line routines, which keeps the
+// code small.
 #define FK_FP_MUL_OUTLINE 1
 #include "launch.h"
 #include "layout.cuh"
@@ -30,13 +42,18 @@ constexpr unsigned long long Z_ABS = 0xd201000000010000ull;
 struct Fp2 {
     Fp c0, c1;
 };
-struct Fp12 {
-    Fp2 c[6];
+struct Fp6 {  // c[0] + c[1] v + c[2] v^2
+    Fp2 c[3];
+};
+struct Fp12 {  // a0 + a1 w; the coefficient of w^k is a0.c[k/2] (k even) or a1.c[k/2] (k odd)
+    Fp6 a0, a1;
 };
 
+// ---------------------------------------------------------------- Fp2
 FK_D void f2_add(Fp2 &r, const Fp2 &a, const Fp2 &b) { f_add(r.c0, a.c0, b.c0); f_add(r.c1, a.c1, b.c1); }
 FK_D void f2_sub(Fp2 &r, const Fp2 &a, const Fp2 &b) { f_sub(r.c0, a.c0, b.c0); f_sub(r.c1, a.c1, b.c1); }
 FK_D void f2_neg(Fp2 &r, const Fp2 &a) { f_neg(r.c0, a.c0); f_neg(r.c1, a.c1); }
+FK_D void f2_conj(Fp2 &r, const Fp2 &a) { r.c0 = a.c0; f_neg(r.c1, a.c1); }
 FK_D bool f2_is_zero(const Fp2 &a) { return f_is_zero(a.c0) && f_is_zero(a.c1); }
 FK_D bool f2_eq(const Fp2 &a, const Fp2 &b) { return f_eq(a.c0, b.c0) && f_eq(a.c1, b.c1); }
 FK_D void f2_zero(Fp2 &r) { f_set_zero(r.c0); f_set_zero(r.c1); }
@@ -48,20 +65,48 @@ FK_D void f2_xi(Fp2 &r, const Fp2 &a) {
     f_add(r.c1, a.c0, a.c1);
     r.c0 = t;
 }
-
+// 3 Fp products; r may alias a or b
 static __device__ __noinline__ void f2_mul(Fp2 *r, const Fp2 *a, const Fp2 *b) {
-    Fp t0, t1, t2, t3;
+    Fp t0, t1, s0, s1;
     fp_mul(t0, a->c0, b->c0);
     fp_mul(t1, a->c1, b->c1);
-    fp_mul(t2, a->c0, b->c1);
-    fp_mul(t3, a->c1, b->c0);
+    f_add(s0, a->c0, a->c1);
+    f_add(s1, b->c0, b->c1);
+    fp_mul(s0, s0, s1);
+    f_sub(s0, s0, t0);
+    f_sub(r->c1, s0, t1);
     f_sub(r->c0, t0, t1);
-    f_add(r->c1, t2, t3);
+}
+// (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
+static __device__ __noinline__ void f2_sqr(Fp2 *r, const Fp2 *a) {
+    Fp s, d, t;
+    f_add(s, a->c0, a->c1);
+    f_sub(d, a->c0, a->c1);
+    fp_mul(t, a->c0, a->c1);
+    fp_mul(r->c0, s, d);
+    f_add(r->c1, t, t);
 }
 FK_D Fp2 f2m(const Fp2 &a, const Fp2 &b) {
     Fp2 r;
     f2_mul(&r, &a, &b);
     return r;
+}
+FK_D Fp2 f2s(const Fp2 &a) {
+    Fp2 r;
+    f2_sqr(&r, &a);
+    return r;
+}
+FK_D void f2_mul_fp(Fp2 &r, const Fp2 &a, const Fp &s) {
+    fp_mul(r.c0, a.c0, s);
+    fp_mul(r.c1, a.c1, s);
+}
+// 12 a (a multiple of 2, 4, 8 by additions)
+FK_D void f2_mul12(Fp2 &r, const Fp2 &a) {
+    Fp2 t4, t8;
+    f2_add(t4, a, a);
+    f2_add(t4, t4, t4);
+    f2_add(t8, t4, t4);
+    f2_add(r, t8, t4);
 }
 // 1 / (a0 + a1 u) = (a0 - a1 u) / (a0^2 + a1^2); inv(0) = 0
 static __device__ __noinline__ void f2_inv(Fp2 *r, const Fp2 *a) {
@@ -75,107 +120,304 @@ static __device__ __noinline__ void f2_inv(Fp2 *r, const Fp2 *a) {
     f_neg(r->c1, t);
 }
 
-FK_D void f12_one(Fp12 &r) {
-    f2_one(r.c[0]);
+// ---------------------------------------------------------------- Fp6
+FK_D void f6_add(Fp6 &r, const Fp6 &a, const Fp6 &b) {
 #pragma unroll 1
-    for (int k = 1; k < 6; k++) f2_zero(r.c[k]);
+    for (int k = 0; k < 3; k++) f2_add(r.c[k], a.c[k], b.c[k]);
+}
+FK_D void f6_sub(Fp6 &r, const Fp6 &a, const Fp6 &b) {
+#pragma unroll 1
+    for (int k = 0; k < 3; k++) f2_sub(r.c[k], a.c[k], b.c[k]);
+}
+FK_D void f6_neg(Fp6 &r, const Fp6 &a) {
+#pragma unroll 1
+    for (int k = 0; k < 3; k++) f2_neg(r.c[k], a.c[k]);
+}
+FK_D void f6_zero(Fp6 &r) {
+#pragma unroll 1
+    for (int k = 0; k < 3; k++) f2_zero(r.c[k]);
+}
+FK_D bool f6_is_zero(const Fp6 &a) { return f2_is_zero(a.c[0]) && f2_is_zero(a.c[1]) && f2_is_zero(a.c[2]); }
+// a v (v^3 = xi); r may alias a
+FK_D void f6_mulv(Fp6 &r, const Fp6 &a) {
+    Fp2 t;
+    f2_xi(t, a.c[2]);
+    r.c[2] = a.c[1];
+    r.c[1] = a.c[0];
+    r.c[0] = t;
+}
+// Karatsuba, 6 Fp2 products; r may alias x or y
+static __device__ __noinline__ void f6_mul(Fp6 *r, const Fp6 *x, const Fp6 *y) {
+    Fp2 t0, t1, t2, s, u, c0, c1;
+    f2_mul(&t0, &x->c[0], &y->c[0]);
+    f2_mul(&t1, &x->c[1], &y->c[1]);
+    f2_mul(&t2, &x->c[2], &y->c[2]);
+    f2_add(s, x->c[1], x->c[2]);  // c0 = t0 + xi ((x1 + x2)(y1 + y2) - t1 - t2)
+    f2_add(u, y->c[1], y->c[2]);
+    f2_mul(&s, &s, &u);
+    f2_sub(s, s, t1);
+    f2_sub(s, s, t2);
+    f2_xi(s, s);
+    f2_add(c0, t0, s);
+    f2_add(s, x->c[0], x->c[1]);  // c1 = (x0 + x1)(y0 + y1) - t0 - t1 + xi t2
+    f2_add(u, y->c[0], y->c[1]);
+    f2_mul(&s, &s, &u);
+    f2_sub(s, s, t0);
+    f2_sub(s, s, t1);
+    f2_xi(u, t2);
+    f2_add(c1, s, u);
+    f2_add(s, x->c[0], x->c[2]);  // c2 = (x0 + x2)(y0 + y2) - t0 - t2 + t1
+    f2_add(u, y->c[0], y->c[2]);
+    f2_mul(&s, &s, &u);
+    f2_sub(s, s, t0);
+    f2_sub(s, s, t2);
+    f2_add(r->c[2], s, t1);
+    r->c[0] = c0;
+    r->c[1] = c1;
+}
+// (t0 + t1 v + t2 v^2) / N with t0 = x0^2 - xi x1 x2, t1 = xi x2^2 - x0 x1,
+// t2 = x1^2 - x0 x2, N = x0 t0 + xi (x2 t1 + x1 t2); inv(0) = 0
+static __device__ __noinline__ void f6_inv(Fp6 *r, const Fp6 *x) {
+    Fp2 t0, t1, t2, s, n;
+    t0 = f2s(x->c[0]);
+    s = f2m(x->c[1], x->c[2]);
+    f2_xi(s, s);
+    f2_sub(t0, t0, s);
+    t1 = f2s(x->c[2]);
+    f2_xi(t1, t1);
+    s = f2m(x->c[0], x->c[1]);
+    f2_sub(t1, t1, s);
+    t2 = f2s(x->c[1]);
+    s = f2m(x->c[0], x->c[2]);
+    f2_sub(t2, t2, s);
+    n = f2m(x->c[2], t1);
+    s = f2m(x->c[1], t2);
+    f2_add(n, n, s);
+    f2_xi(n, n);
+    s = f2m(x->c[0], t0);
+    f2_add(n, n, s);
+    f2_inv(&n, &n);
+    r->c[0] = f2m(t0, n);
+    r->c[1] = f2m(t1, n);
+    r->c[2] = f2m(t2, n);
+}
+
+// ---------------------------------------------------------------- Fp12
+FK_D void f12_one(Fp12 &r) {
+    f6_zero(r.a0);
+    f6_zero(r.a1);
+    f2_one(r.a0.c[0]);
 }
 FK_D bool f12_is_one(const Fp12 &a) {
     Fp2 one;
     f2_one(one);
-    bool ok = f2_eq(a.c[0], one);
-#pragma unroll 1
-    for (int k = 1; k < 6; k++) ok &= f2_is_zero(a.c[k]);
-    return ok;
+    return f2_eq(a.a0.c[0], one) && f2_is_zero(a.a0.c[1]) && f2_is_zero(a.a0.c[2]) && f6_is_zero(a.a1);
 }
-
-// r = a b in Fp2[w]/(w^6 - xi); r may alias a or b
+// f^(p^6): the conjugate over Fp6 (the inverse in the cyclotomic subgroup)
+FK_D void f12_conj(Fp12 &r, const Fp12 &a) {
+    r.a0 = a.a0;
+    f6_neg(r.a1, a.a1);
+}
+// 3 Fp6 products; r may alias a or b
 static __device__ __noinline__ void f12_mul(Fp12 *r, const Fp12 *a, const Fp12 *b) {
-    Fp2 t[11];
-#pragma unroll 1
-    for (int k = 0; k < 11; k++) f2_zero(t[k]);
-#pragma unroll 1
-    for (int i = 0; i < 6; i++) {
-#pragma unroll 1
-        for (int j = 0; j < 6; j++) {
-            Fp2 p;
-            f2_mul(&p, &a->c[i], &b->c[j]);
-            f2_add(t[i + j], t[i + j], p);
-        }
+    Fp6 t0, t1, s, u;
+    f6_mul(&t0, &a->a0, &b->a0);
+    f6_mul(&t1, &a->a1, &b->a1);
+    f6_add(s, a->a0, a->a1);
+    f6_add(u, b->a0, b->a1);
+    f6_mul(&s, &s, &u);
+    f6_sub(s, s, t0);
+    f6_sub(r->a1, s, t1);
+    f6_mulv(t1, t1);
+    f6_add(r->a0, t0, t1);
+}
+// (a0 + a1 w)^2 = ((a0 + a1)(a0 + v a1) - t - v t) + 2 t w, t = a0 a1: 2 Fp6 products
+static __device__ __noinline__ void f12_sqr(Fp12 *r, const Fp12 *a) {
+    Fp6 t, s, u;
+    f6_mul(&t, &a->a0, &a->a1);
+    f6_add(s, a->a0, a->a1);
+    f6_mulv(u, a->a1);
+    f6_add(u, a->a0, u);
+    f6_mul(&s, &s, &u);
+    f6_sub(s, s, t);
+    f6_mulv(u, t);
+    f6_sub(r->a0, s, u);
+    f6_add(r->a1, t, t);
+}
+// (a0 + a1 w)^-1 = (a0 - a1 w) / (a0^2 - v a1^2)
+static __device__ __noinline__ void f12_inv(Fp12 *r, const Fp12 *a) {
+    Fp6 s, t;
+    f6_mul(&s, &a->a0, &a->a0);
+    f6_mul(&t, &a->a1, &a->a1);
+    f6_mulv(t, t);
+    f6_sub(s, s, t);
+    f6_inv(&s, &s);
+    f6_mul(&r->a0, &a->a0, &s);
+    f6_neg(t, a->a1);
+    f6_mul(&r->a1, &t, &s);
+}
+FK_D void frob_coef(Fp2 &g, const uint32_t (*c)[12]) {
+#pragma unroll
+    for (int i = 0; i < 12; i++) {
+        g.c0.w[i] = c[0][i];
+        g.c1.w[i] = c[1][i];
     }
+}
+// a^p (conj = true, coefficients c_frob1) or a^(p^2) (conj = false, c_frob2):
+// sum_k a_k^(p^j) g_k w^k
+static __device__ __noinline__ void f12_frob(Fp12 *r, const Fp12 *a, bool conj) {
+    const uint32_t(*tab)[2][12] = conj ? c_frob1 : c_frob2;
 #pragma unroll 1
-    for (int k = 0; k < 5; k++) {  // w^(k+6) = xi w^k
-        Fp2 x;
-        f2_xi(x, t[k + 6]);
-        f2_add(r->c[k], t[k], x);
+    for (int k = 0; k < 6; k++) {
+        const Fp2 &src = (k & 1) ? a->a1.c[k >> 1] : a->a0.c[k >> 1];
+        Fp2 &dst = (k & 1) ? r->a1.c[k >> 1] : r->a0.c[k >> 1];
+        Fp2 x, g;
+        if (conj) f2_conj(x, src);
+        else x = src;
+        frob_coef(g, tab[k]);
+        f2_mul(&dst, &x, &g);
     }
-    r->c[5] = t[5];
 }
 
-// the line through T with twist slope lam, evaluated at P = (xp, yp), times w^3
-FK_D void line(Fp12 &l, const Fp2 &lam, const Fp2 &xt, const Fp2 &yt, const Fp &xp, const Fp &yp) {
-#pragma unroll 1
-    for (int k = 0; k < 6; k++) f2_zero(l.c[k]);
-    Fp2 t = f2m(lam, xt);
-    f2_sub(l.c[0], t, yt);
-    Fp q;
-    fp_mul(q, lam.c0, xp);
-    f_neg(l.c[2].c0, q);
-    fp_mul(q, lam.c1, xp);
-    f_neg(l.c[2].c1, q);
-    l.c[3].c0 = yp;
+// ---------------------------------------------------------------- Miller loop
+struct G2H {  // homogeneous projective point of the twist
+    Fp2 x, y, z;
+};
+// the line c0 + c2 w^2 + c3 w^3 as an Fp12 element
+FK_D void line_f12(Fp12 &l, const Fp2 &c0, const Fp2 &c2, const Fp2 &c3) {
+    f6_zero(l.a0);
+    f6_zero(l.a1);
+    l.a0.c[0] = c0;
+    l.a0.c[1] = c2;
+    l.a1.c[1] = c3;
 }
-
-// f = f^(2^63) * Miller function of (P, Q) (f = 1 gives the Miller value); P and Q affine, not infinity
-static __device__ __noinline__ void miller(Fp12 *f, const Fp *xp, const Fp *yp, const Fp2 *xq, const Fp2 *yq) {
-    Fp2 xt = *xq, yt = *yq, lam, t, u;
+// T = 2T; l = tangent at T evaluated at P
+static __device__ __noinline__ void dbl_step(G2H *T, Fp12 *l, const Fp *xp, const Fp *yp) {
+    Fp2 B = f2s(T->y), C = f2s(T->z), E, F, XX = f2s(T->x), H, t, u, c2, c3;
+    f2_xi(t, C);
+    f2_mul12(E, t);  // 3 b' Z^2 = 12 xi Z^2
+    f2_add(F, E, E);
+    f2_add(F, F, E);  // 3 E
+    H = f2m(T->y, T->z);
+    f2_add(H, H, H);  // 2 Y Z
+    f2_sub(t, B, E);
+    f2_add(u, XX, XX);
+    f2_add(u, u, XX);
+    f2_mul_fp(c2, u, *xp);
+    f2_neg(c2, c2);
+    f2_mul_fp(c3, H, *yp);
+    line_f12(*l, t, c2, c3);
+    t = f2m(T->x, T->y);
+    f2_add(t, t, t);
+    f2_sub(u, B, F);
+    T->x = f2m(t, u);  // 2 X Y (B - F)
+    f2_add(t, B, F);
+    T->y = f2s(t);
+    u = f2s(E);
+    f2_mul12(u, u);
+    f2_sub(T->y, T->y, u);  // (B + F)^2 - 12 E^2
+    t = f2m(B, H);
+    f2_add(t, t, t);
+    f2_add(T->z, t, t);  // 4 B H
+}
+// T = T + Q (Q affine); l = chord through T and Q evaluated at P
+static __device__ __noinline__ void add_step(G2H *T, Fp12 *l, const Fp2 *xq, const Fp2 *yq, const Fp *xp,
+                                             const Fp *yp) {
+    Fp2 th, la, t, u, c0, c2, c3, C, D, E, F, G, H;
+    t = f2m(*yq, T->z);
+    f2_sub(th, T->y, t);
+    t = f2m(*xq, T->z);
+    f2_sub(la, T->x, t);
+    t = f2m(th, *xq);
+    u = f2m(la, *yq);
+    f2_sub(c0, t, u);
+    f2_mul_fp(c2, th, *xp);
+    f2_neg(c2, c2);
+    f2_mul_fp(c3, la, *yp);
+    line_f12(*l, c0, c2, c3);
+    C = f2s(th);
+    D = f2s(la);
+    E = f2m(la, D);
+    F = f2m(T->z, C);
+    G = f2m(T->x, D);
+    f2_add(H, E, F);
+    f2_sub(H, H, G);
+    f2_sub(H, H, G);
+    T->x = f2m(la, H);
+    f2_sub(t, G, H);
+    t = f2m(th, t);
+    u = f2m(T->y, E);
+    f2_sub(T->y, t, u);
+    T->z = f2m(T->z, E);
+}
+// f = prod over the n (<= 2) pairs of their Miller values (P affine over Fp,
+// Q affine on the twist, neither infinity)
+static __device__ __noinline__ void miller(Fp12 *f, int n, const Fp *xp, const Fp *yp, const Fp2 *xq, const Fp2 *yq) {
+    G2H T[2];
     Fp12 l;
 #pragma unroll 1
+    for (int j = 0; j < n; j++) {
+        T[j].x = xq[j];
+        T[j].y = yq[j];
+        f2_one(T[j].z);
+    }
+    f12_one(*f);
+#pragma unroll 1
     for (int i = 62; i >= 0; i--) {
-        // tangent at T: lam = 3 xT^2 / (2 yT)
-        t = f2m(xt, xt);
-        f2_add(u, t, t);
-        f2_add(t, u, t);
-        f2_add(u, yt, yt);
-        f2_inv(&u, &u);
-        lam = f2m(t, u);
-        line(l, lam, xt, yt, *xp, *yp);
-        f12_mul(f, f, f);
-        f12_mul(f, f, &l);
-        t = f2m(lam, lam);
-        f2_sub(t, t, xt);
-        f2_sub(t, t, xt);  // x3
-        f2_sub(u, xt, t);
-        u = f2m(lam, u);
-        f2_sub(yt, u, yt);
-        xt = t;
-        if ((Z_ABS >> i) & 1ull) {  // chord through T and Q
-            f2_sub(t, *yq, yt);
-            f2_sub(u, *xq, xt);
-            f2_inv(&u, &u);
-            lam = f2m(t, u);
-            line(l, lam, xt, yt, *xp, *yp);
+        f12_sqr(f, f);
+#pragma unroll 1
+        for (int j = 0; j < n; j++) {
+            dbl_step(&T[j], &l, &xp[j], &yp[j]);
             f12_mul(f, f, &l);
-            t = f2m(lam, lam);
-            f2_sub(t, t, xt);
-            f2_sub(t, t, *xq);
-            f2_sub(u, xt, t);
-            u = f2m(lam, u);
-            f2_sub(yt, u, yt);
-            xt = t;
+        }
+        if ((Z_ABS >> i) & 1ull) {
+#pragma unroll 1
+            for (int j = 0; j < n; j++) {
+                add_step(&T[j], &l, &xq[j], &yq[j], &xp[j], &yp[j]);
+                f12_mul(f, f, &l);
+            }
         }
     }
 }
 
-static __device__ __noinline__ void final_exp(Fp12 *r, const Fp12 *f) {
-    Fp12 acc;
-    f12_one(acc);
+// ---------------------------------------------------------------- final exponentiation
+// r = a^z (z = -|z| < 0, a in the cyclotomic subgroup, where the inverse is
+// the conjugate); r may alias a
+static __device__ __noinline__ void exp_z(Fp12 *r, const Fp12 *a) {
+    Fp12 acc = *a;
 #pragma unroll 1
-    for (int b = FINAL_EXP_BITS - 1; b >= 0; b--) {
-        f12_mul(&acc, &acc, &acc);
-        if ((c_final_exp[b >> 6] >> (b & 63)) & 1ull) f12_mul(&acc, &acc, f);
+    for (int i = 62; i >= 0; i--) {
+        f12_sqr(&acc, &acc);
+        if ((Z_ABS >> i) & 1ull) f12_mul(&acc, &acc, a);
     }
-    *r = acc;
+    f12_conj(*r, acc);
+}
+// r = f^(3 (p^12 - 1) / r)
+static __device__ __noinline__ void final_exp(Fp12 *r, const Fp12 *f) {
+    Fp12 m, t, a, b, c;
+    f12_inv(&t, f);  // easy part: m = f^((p^6 - 1)(p^2 + 1))
+    f12_conj(m, *f);
+    f12_mul(&m, &m, &t);
+    f12_frob(&t, &m, false);
+    f12_mul(&m, &t, &m);
+    exp_z(&a, &m);  // a = m^(z - 1)
+    f12_conj(t, m);
+    f12_mul(&a, &a, &t);
+    exp_z(&t, &a);  // a = a^(z - 1)
+    f12_conj(a, a);
+    f12_mul(&a, &t, &a);
+    exp_z(&b, &a);  // b = a^(z + p)
+    f12_frob(&t, &a, true);
+    f12_mul(&b, &b, &t);
+    exp_z(&c, &b);  // c = b^(z^2 + p^2 - 1)
+    exp_z(&c, &c);
+    f12_frob(&t, &b, false);
+    f12_mul(&c, &c, &t);
+    f12_conj(t, b);
+    f12_mul(&c, &c, &t);
+    f12_sqr(&t, &m);  // times m^3
+    f12_mul(&t, &t, &m);
+    f12_mul(r, &c, &t);
 }
 
 // ---------------------------------------------------------------- conversions
@@ -278,21 +520,17 @@ __global__ void __launch_bounds__(64) k_pairing(int op, uint64_t *out, uint8_t *
                                                 size_t count) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= count) return;
-    Fp12 f;
-    f12_one(f);
-    Fp xp, yp;
-    Fp2 xq, yq;
-    if (g1_affine(xp, yp, a + 18 * i) && g2_affine(xq, yq, b + 36 * i)) miller(&f, &xp, &yp, &xq, &yq);
-    if (op == 1 && g1_affine(xp, yp, c + 18 * i) && g2_affine(xq, yq, d + 36 * i)) {
-        // e(c, d)^-1 = e(-c, d); the loop squares its accumulator, so the
-        // second Miller value starts from 1 and joins f by one product
-        Fp12 g;
-        f12_one(g);
-        f_neg(yp, yp);
-        miller(&g, &xp, &yp, &xq, &yq);
-        f12_mul(&f, &f, &g);
+    Fp xp[2], yp[2];
+    Fp2 xq[2], yq[2];
+    int n = 0;
+    if (g1_affine(xp[n], yp[n], a + 18 * i) && g2_affine(xq[n], yq[n], b + 36 * i)) n++;
+    if (op == 1 && g1_affine(xp[n], yp[n], c + 18 * i) && g2_affine(xq[n], yq[n], d + 36 * i)) {
+        f_neg(yp[n], yp[n]);  // e(c, d)^-1 = e(-c, d)
+        n++;
     }
-    Fp12 e;
+    Fp12 f, e;
+    if (n) miller(&f, n, xp, yp, xq, yq);
+    else f12_one(f);
     final_exp(&e, &f);
     if (op == 1) {
         ok[i] = f12_is_one(e) ? 1 : 0;
@@ -300,8 +538,9 @@ __global__ void __launch_bounds__(64) k_pairing(int op, uint64_t *out, uint8_t *
     }
 #pragma unroll 1
     for (int k = 0; k < 6; k++) {
-        fp_to_words(out + 72 * i + 12 * k, e.c[k].c0);
-        fp_to_words(out + 72 * i + 12 * k + 6, e.c[k].c1);
+        const Fp2 &v = (k & 1) ? e.a1.c[k >> 1] : e.a0.c[k >> 1];
+        fp_to_words(out + 72 * i + 12 * k, v.c0);
+        fp_to_words(out + 72 * i + 12 * k + 6, v.c1);
     }
 }
 

@@ -223,15 +223,16 @@ int fk20_ctx_batch_proofs(fk20_ctx *ctx, uint8_t *proofs, const fr_t *polys, uns
  * homogeneous projective in standard form, infinity written as (0, 1, 0).
  * The pairing is the optimal ate pairing of BLS12 curves (up to a fixed
  * exponent: non-degenerate and bilinear, which is what the checks use).  One
- * thread per check; a launch takes about 1.2 s whatever its count up to ~10^4
- * checks (B200): for verification, not proving. */
+ * thread per check; a launch takes about 44 ms whatever its count up to ~10^4
+ * checks (B200; 212 k checks/s at 9,472). */
 typedef struct { fp_t x[2], y[2], z[2]; } g2p_t;
 
 /* ok[i] = (e(a[i], b[i]) == e(c[i], d[i])); a KZG multiproof check is
  * e(C - [I(s)]G1, G2) == e(proof, [s^l - x^l]G2). */
 int fk20_pairing_check_n(uint8_t *ok, const g1p_t *a, const g2p_t *b, const g1p_t *c, const g2p_t *d, size_t count,
                          void *stream);
-/* out[i][12] = e(a[i], b[i]) as the 6 Fp2 coefficients of w in Fp12 = Fp2[w]/(w^6 - (1 + u)) */
+/* out[i][12] = e(a[i], b[i]) as the 6 Fp2 coefficients of w in Fp12 = Fp2[w]/(w^6 - (1 + u)): the
+ * Miller value over |z| with the final exponent 3 (p^12 - 1)/r */
 int fk20_pairing_n(fp_t *out, const g1p_t *a, const g2p_t *b, size_t count, void *stream);
 /* G2 element-wise: 0 add, 1 dbl, 2 neg, 3 sub, 4 mul by fr_t scalar (b), 5 normalise,
  * 6 on-curve flag (b: uint8 out). */
