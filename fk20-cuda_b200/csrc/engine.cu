@@ -334,6 +334,7 @@ struct fk20_ctx {
     } commit;
     Workspace ws;   // the context's own calls
     DevBuf D2, scratch, xext, fp_dev;
+    DevBuf verify;  // check_proof_multi intermediates
     Profiler prof;
 };
 
@@ -849,6 +850,7 @@ int fk20_ctx_destroy(fk20_ctx *ctx) {
         ctx->scratch.release();
         ctx->xext.release();
         ctx->fp_dev.release();
+        ctx->verify.release();
     }
     delete ctx;
     return 0;
@@ -1437,6 +1439,39 @@ int fk20_pairing_check_n(uint8_t *ok, const g1p_t *a, const g2p_t *b, const g1p_
     CKR(current_device_ready());
     launch_pairing(1, nullptr, ok, (const uint64_t *)a, (const uint64_t *)b, (const uint64_t *)c,
                    (const uint64_t *)d, count, S_(stream));
+    CKL();
+    return 0;
+}
+
+int fk20_ctx_check_proof_multi(fk20_ctx *ctx, uint8_t *ok, const g1p_t *commitment, const g1p_t *proof,
+                               const fr_t *x, const fr_t *ys, unsigned l, const g2p_t *setup_g2, unsigned count,
+                               void *stream) {
+    if (!ctx || !ok || !commitment || !proof || !x || !ys || !setup_g2) return FK20_EINVAL;
+    if (count == 0 || count > MAX_ROWS || l == 0 || l > COMMIT_CHUNK || (l & (l - 1))) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    if (ctx->commit.n < (int)COMMIT_CHUNK) return FK20_ENOSETUP;
+    int log_l = 0;
+    while ((1u << log_l) < l) log_l++;
+    const int G = (int)((count + 31) / 32);
+    const size_t poly_b = (size_t)count * COMMIT_CHUNK * sizeof(fr_t), xl_b = (size_t)count * sizeof(fr_t),
+                 pt_b = (size_t)count * sizeof(g1p_t);
+    CKR(ctx->verify.reserve(poly_b + xl_b + 3 * pt_b));
+    CKR(ctx->commit.part.reserve(tile_bytes(G, 1)));
+    char *base = (char *)ctx->verify.p;
+    uint64_t *poly = (uint64_t *)base, *xl = (uint64_t *)(base + poly_b);
+    uint64_t *I = (uint64_t *)(base + poly_b + xl_b), *T = I + 18 * (size_t)count, *A = T + 18 * (size_t)count;
+    const cudaStream_t st = S_(stream);
+    // I(X) over the coset and x^l; [I(s)]G1 with the commitment tables
+    launch_interp(poly, xl, (const uint64_t *)x, (const uint64_t *)ys, log_l, count, st);
+    launch_commit(I, (uint4 *)ctx->commit.part.p, poly, (const uint4 *)ctx->commit.table.p, (int)count,
+                  (int)COMMIT_CHUNK, ctx->commit.W, ctx->commit.cb, st);
+    // e(C - [I(s)] + [x^l] proof, G2) == e(proof, [s^l]G2)
+    launch_g1_op(4, T, (const uint64_t *)proof, xl, count, st);
+    launch_g1_op(3, A, (const uint64_t *)commitment, I, count, st);
+    launch_g1_op(0, I, A, T, count, st);
+    launch_pairing(1, nullptr, ok, I, (const uint64_t *)setup_g2, (const uint64_t *)proof,
+                   (const uint64_t *)(setup_g2 + l), count, st, 3);
     CKL();
     return 0;
 }

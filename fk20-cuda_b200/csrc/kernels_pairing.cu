@@ -514,17 +514,19 @@ static __device__ __noinline__ void g2_add(Fp2 *xr, Fp2 *yr, bool *ir, Fp2 x1, F
 
 // ---------------------------------------------------------------- kernels
 // op 0: out[i] = e(a[i], b[i]) (12 fp_t: the 6 Fp2 coefficients of w);
-// op 1: ok[i] = e(a[i], b[i]) == e(c[i], d[i])
+// op 1: ok[i] = e(a[i], b[i]) == e(c[i], d[i]).
+// bcast bit 0: b is one point for every i; bit 1: d likewise.
 __global__ void __launch_bounds__(64) k_pairing(int op, uint64_t *out, uint8_t *ok, const uint64_t *a,
                                                 const uint64_t *b, const uint64_t *c, const uint64_t *d,
-                                                size_t count) {
+                                                size_t count, int bcast) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= count) return;
+    const size_t ib = (bcast & 1) ? 0 : i, id = (bcast & 2) ? 0 : i;
     Fp xp[2], yp[2];
     Fp2 xq[2], yq[2];
     int n = 0;
-    if (g1_affine(xp[n], yp[n], a + 18 * i) && g2_affine(xq[n], yq[n], b + 36 * i)) n++;
-    if (op == 1 && g1_affine(xp[n], yp[n], c + 18 * i) && g2_affine(xq[n], yq[n], d + 36 * i)) {
+    if (g1_affine(xp[n], yp[n], a + 18 * i) && g2_affine(xq[n], yq[n], b + 36 * ib)) n++;
+    if (op == 1 && g1_affine(xp[n], yp[n], c + 18 * i) && g2_affine(xq[n], yq[n], d + 36 * id)) {
         f_neg(yp[n], yp[n]);  // e(c, d)^-1 = e(-c, d)
         n++;
     }
@@ -542,6 +544,56 @@ __global__ void __launch_bounds__(64) k_pairing(int op, uint64_t *out, uint8_t *
         fp_to_words(out + 72 * i + 12 * k, v.c0);
         fp_to_words(out + 72 * i + 12 * k + 6, v.c1);
     }
+}
+
+// Interpolation for check_proof_multi (FK20Py/kzg_proofs.py:214-217): from the
+// evaluations ys[k] = f(x w^k), k < l (w = w_l), the coefficients of the
+// interpolation polynomial I(X) = sum_j c_j X^j, c_j = (1/l) sum_k ys[k] w^-jk
+// / x^j, written as poly[32 i + j] (zero above l), and xl[i] = x^l.  Fr in
+// Montgomery form inside; fr_t standard form (any representative) in,
+// canonical out.
+__global__ void __launch_bounds__(64) k_interp(uint64_t *poly, uint64_t *xl, const uint64_t *x, const uint64_t *ys,
+                                               int log_l, size_t count) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int l = 1 << log_l, step = 32 >> log_l;
+    Fr y[32], xm, xinv, t, acc, w, s;
+#pragma unroll 1
+    for (int k = 0; k < l; k++) {
+        fr_from_ref(t, ys + 4 * ((size_t)l * i + k));
+        f_to_mont(y[k], t);
+    }
+    fr_from_ref(t, x + 4 * i);
+    f_to_mont(xm, t);
+    f_inv(xinv, xm);
+#pragma unroll
+    for (int q = 0; q < 8; q++) s.w[q] = c_inv_pow2[log_l][q];  // s = (1/l) x^-j, from j = 0
+#pragma unroll 1
+    for (int j = 0; j < 32; j++) {
+        uint64_t *dst = poly + 4 * (32 * i + j);
+        if (j >= l) {
+            dst[0] = dst[1] = dst[2] = dst[3] = 0;
+            continue;
+        }
+        f_set_zero(acc);
+#pragma unroll 1
+        for (int k = 0; k < l; k++) {
+            const int e = (j * k * step) & 31;
+#pragma unroll
+            for (int q = 0; q < 8; q++) w.w[q] = c_w32_inv[e][q];
+            f_mul(t, y[k], w);
+            f_add(acc, acc, t);
+        }
+        f_mul(acc, acc, s);
+        f_from_mont(t, acc);
+        fr_to_ref(dst, t);
+        f_mul(s, s, xinv);
+    }
+    t = xm;
+#pragma unroll 1
+    for (int q = 0; q < log_l; q++) f_mul(t, t, t);
+    f_from_mont(acc, t);
+    fr_to_ref(xl + 4 * i, acc);
 }
 
 // G2 element-wise: 0 add, 1 dbl, 2 neg, 3 sub, 4 mul by fr_t scalar, 5 normalize,
@@ -598,8 +650,12 @@ __global__ void __launch_bounds__(64) k_g2_op(int op, uint64_t *out, const uint6
 }
 
 void launch_pairing(int op, uint64_t *out, uint8_t *ok, const uint64_t *a, const uint64_t *b, const uint64_t *c,
-                    const uint64_t *d, size_t count, cudaStream_t st) {
-    k_pairing<<<blocks_for(count, 64), 64, 0, st>>>(op, out, ok, a, b, c, d, count);
+                    const uint64_t *d, size_t count, cudaStream_t st, int bcast) {
+    k_pairing<<<blocks_for(count, 64), 64, 0, st>>>(op, out, ok, a, b, c, d, count, bcast);
+}
+void launch_interp(uint64_t *poly, uint64_t *xl, const uint64_t *x, const uint64_t *ys, int log_l, size_t count,
+                   cudaStream_t st) {
+    k_interp<<<blocks_for(count, 64), 64, 0, st>>>(poly, xl, x, ys, log_l, count);
 }
 void launch_g2_op(int op, uint64_t *out, const uint64_t *a, const void *b, size_t count, cudaStream_t st) {
     k_g2_op<<<blocks_for(count, 64), 64, 0, st>>>(op, out, a, b, count);

@@ -91,7 +91,9 @@ void launch_tile_to_proofs(uint8_t *out, const uint4 *D, const size_t *out_off, 
 
 // kernels_pairing.cu: op 0 pairing values, op 1 pairing checks; G2 element-wise ops
 void launch_pairing(int op, uint64_t *out, uint8_t *ok, const uint64_t *a, const uint64_t *b, const uint64_t *c,
-                    const uint64_t *d, size_t count, cudaStream_t st);
+                    const uint64_t *d, size_t count, cudaStream_t st, int bcast = 0);
+void launch_interp(uint64_t *poly, uint64_t *xl, const uint64_t *x, const uint64_t *ys, int log_l, size_t count,
+                   cudaStream_t st);
 void launch_g2_op(int op, uint64_t *out, const uint64_t *a, const void *b, size_t count, cudaStream_t st);
 
 // kernels_tables.cu

@@ -42,6 +42,7 @@ ABI_SYMBOLS = (
     "fk20_server_wait", "fk20_server_get_stats", "fk20_server_reset_stats", "fk20_server_destroy",
     "fk20_g1p_compress_n", "fk20_h_fft2proofs", "fk20_ctx_poly2proofs", "fk20_ctx_batch_proofs",
     "fk20_ctx_load_commit", "fk20_ctx_commit", "fk20_pairing_check_n", "fk20_pairing_n", "g2p_op_n",
+    "fk20_ctx_check_proof_multi",
 )
 
 # kernel kinds of the per-launch profiler (FK20_K_* in the header)
@@ -159,6 +160,7 @@ def lib() -> ctypes.CDLL:
             "fk20_ctx_load_commit": ([vp, u, vp, i, vp], i),
             "fk20_ctx_commit": ([vp, vp, vp, u, u, vp], i),
             "fk20_pairing_check_n": ([vp, vp, vp, vp, vp, sz, vp], i),
+            "fk20_ctx_check_proof_multi": ([vp, vp, vp, vp, vp, vp, u, vp, u, vp], i),
             "fk20_pairing_n": ([vp, vp, vp, sz, vp], i),
             "g2p_op_n": ([i, vp, vp, vp, sz, vp], i),
         }
@@ -245,6 +247,13 @@ class Context:
     def commit(self, commitments, poly, rows: int, n: int):
         """commitments[rows] (g1p_t) = sum_i poly[row][i] * setup_i."""
         call("fk20_ctx_commit", self.h, _ptr(commitments), _ptr(poly), rows, n, _stream())
+
+    def check_proof_multi(self, ok, commitments, proofs, x, ys, l: int, setup_g2, count: int):
+        """ok[count] (uint8) = check_proof_multi of each (commitment, proof, x,
+        ys[l]); setup_g2 = [s^k]G2 for k = 0..l (g2p_t rows).  Needs the
+        commitment tables (load_commit with n >= 32)."""
+        call("fk20_ctx_check_proof_multi", self.h, _ptr(ok), _ptr(commitments), _ptr(proofs), _ptr(x), _ptr(ys), l,
+             _ptr(setup_g2), count, _stream())
 
     def poly2proofs(self, proofs, poly, rows: int, n: int):
         """proofs: uint8 CUDA tensor [rows][2n/16][48], data-availability order."""

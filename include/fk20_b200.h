@@ -231,6 +231,19 @@ typedef struct { fp_t x[2], y[2], z[2]; } g2p_t;
  * e(C - [I(s)]G1, G2) == e(proof, [s^l - x^l]G2). */
 int fk20_pairing_check_n(uint8_t *ok, const g1p_t *a, const g2p_t *b, const g1p_t *c, const g2p_t *d, size_t count,
                          void *stream);
+/* check_proof_multi (FK20Py/kzg_proofs.py:207-232) for count proofs at once:
+ * ok[i] = 1 when proof[i] proves f(x[i] w^k) = ys[l i + k] for k < l (w = the
+ * l-th root of unity 5^((r-1)/l), l a power of two <= 32) for the polynomial
+ * committed in commitment[i]; else 0.  The G1 half of the setup comes from
+ * the context's commitment tables (fk20_ctx_load_commit, n >= 32);
+ * setup_g2 holds [s^k]G2 for k = 0..l (device memory, as the reference's
+ * setup[1]).  The check is e(C - [I(s)]G1 + [x^l] proof, G2) ==
+ * e(proof, [s^l]G2), I the interpolation polynomial of ys over the coset:
+ * the reference's equation with x^l moved from G2 to G1.  All pointers are
+ * device memory; count <= 2^20. */
+int fk20_ctx_check_proof_multi(fk20_ctx *ctx, uint8_t *ok, const g1p_t *commitment, const g1p_t *proof,
+                               const fr_t *x, const fr_t *ys, unsigned l, const g2p_t *setup_g2, unsigned count,
+                               void *stream);
 /* out[i][12] = e(a[i], b[i]) as the 6 Fp2 coefficients of w in Fp12 = Fp2[w]/(w^6 - (1 + u)): the
  * Miller value over |z| with the final exponent 3 (p^12 - 1)/r */
 int fk20_pairing_n(fp_t *out, const g1p_t *a, const g2p_t *b, size_t count, void *stream);

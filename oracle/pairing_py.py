@@ -137,3 +137,52 @@ def pairing_check(p1, q1, p2, q2) -> bool:
     if p2 is not None and q2 is not None:
         f = f12mul(f, miller((p2[0], (-p2[1]) % P), q2))
     return f12pow(f, FINAL_EXP) == ONE12
+
+
+# ---------------------------------------------------------------- G1 (affine over Fp) and check_proof_multi
+def g1add(p, q):
+    if p is None:
+        return q
+    if q is None:
+        return p
+    if p[0] == q[0]:
+        if (p[1] + q[1]) % P == 0:
+            return None
+        lam = 3 * p[0] * p[0] * pow(2 * p[1], P - 2, P) % P
+    else:
+        lam = (q[1] - p[1]) * pow(q[0] - p[0], P - 2, P) % P
+    x3 = (lam * lam - p[0] - q[0]) % P
+    return (x3, (lam * (p[0] - x3) - p[1]) % P)
+
+
+def g1mul(k, p):
+    r = None
+    for bit in bin(k % R)[2:]:
+        r = g1add(r, r)
+        if bit == "1":
+            r = g1add(r, p)
+    return r
+
+
+def g1neg(p):
+    return None if p is None else (p[0], (-p[1]) % P)
+
+
+def check_proof_multi(commitment, proof, x, ys, setup_g1, setup_g2):
+    """FK20Py/kzg_proofs.py:207-232: the proof that f(x w^i) = ys[i], i < n
+    (w the n-th root of unity 5^((r-1)/n)), for the polynomial committed in
+    `commitment`; setup_g1 / setup_g2 = [s^k]G1 / [s^k]G2.  Affine points
+    (None = infinity), field elements as ints."""
+    n = len(ys)
+    w = pow(5, (R - 1) // n, R)
+    inv_n, inv_x = pow(n, R - 2, R), pow(x, R - 2, R)
+    # interpolation over the coset: inverse DFT of ys, then coefficient i / x^i
+    interp = [sum(ys[k] * pow(w, (R - 1 - j * k) % (R - 1), R) for k in range(n)) * inv_n % R for j in range(n)]
+    interp = [c * pow(inv_x, i, R) % R for i, c in enumerate(interp)]
+    xn_minus_yn = g2add(setup_g2[n], g2mul((R - pow(x, n, R)) % R, setup_g2[0]))
+    lincomb = None
+    for pt, c in zip(setup_g1, interp):
+        lincomb = g1add(lincomb, g1mul(c, pt))
+    com_minus_interp = g1add(commitment, g1neg(lincomb))
+    # e(C - I(s), G2) == e(proof, [s^n - x^n]G2)
+    return pairing_check(com_minus_interp, setup_g2[0], proof, xn_minus_yn)

@@ -46,3 +46,29 @@ def engine():
     import fk20b200
     fk20b200.lib()
     return fk20b200
+
+
+def kzg_multi_case(l=4, deg=8, tau=0x5EED5EED1234567, seed=77):
+    """A small check_proof_multi case built from the KZG definitions, with tau
+    known: f, x, ys[k] = f(x w^k), the commitment [f(tau)]G1 and the proof
+    [q(tau)]G1, q = (f - I) / (X^l - x^l), I = f mod (X^l - x^l)."""
+    import random
+    import oracle as O
+    import pairing_py as PP
+    rnd = random.Random(seed)
+    R = O.R
+    f = [rnd.randrange(R) for _ in range(deg)]
+    x = rnd.randrange(1, R)
+    w = pow(5, (R - 1) // l, R)
+    ev = lambda z: sum(c * pow(z, i, R) for i, c in enumerate(f)) % R
+    ys = [ev(x * pow(w, k, R) % R) for k in range(l)]
+    xl = pow(x, l, R)
+    rem = [sum(f[k + l * q] * pow(xl, q, R) for q in range((deg - k + l - 1) // l)) % R for k in range(l)]
+    i_tau = sum(c * pow(tau, k, R) for k, c in enumerate(rem)) % R
+    q_tau = (ev(tau) - i_tau) * pow((pow(tau, l, R) - xl) % R, R - 2, R) % R
+    g = O.g1_generator()
+    G1 = (O.limbs_to_int(g[0:6]), O.limbs_to_int(g[6:12]))
+    G2 = PP.g2_generator()
+    return dict(f=f, x=x, ys=ys, tau=tau, commitment=PP.g1mul(ev(tau), G1), proof=PP.g1mul(q_tau, G1),
+                setup_g1=[PP.g1mul(pow(tau, k, R), G1) for k in range(l)],
+                setup_g2=[PP.g2mul(pow(tau, k, R), G2) for k in range(l + 1)])

@@ -8,7 +8,7 @@ import pytest
 
 import oracle as O
 import pairing_py as PP
-from conftest import fk20_setup_data
+from conftest import fk20_setup_data, kzg_multi_case
 
 pytestmark = pytest.mark.gpu
 
@@ -146,4 +146,83 @@ def test_fk20_proofs_verify_as_kzg_multiproofs(engine):
     engine.call("fk20_pairing_check_n", engine._ptr(ok), engine._ptr(A), engine._ptr(B), engine._ptr(proofs),
                 engine._ptr(rhs2), 2 * len(js), engine._stream())
     assert ok.cpu().numpy().tolist() == [1] * len(js) + [0] * len(js)
+    c.close()
+
+
+def g1_to_array(pts):
+    """affine python G1 points -> g1p_t rows (z = 1)"""
+    out = np.zeros((len(pts), 18), np.uint64)
+    for i, q in enumerate(pts):
+        out[i, 0:6] = O.int_to_limbs(q[0], 6)
+        out[i, 6:12] = O.int_to_limbs(q[1], 6)
+        out[i, 12] = 1
+    return out
+
+
+def test_check_proof_multi_on_engine_proofs(engine):
+    """fk20_ctx_check_proof_multi (check_proof_multi, FK20Py/kzg_proofs.py:207-232)
+    on the engine's own proofs: h_fft[j] proves the coset x w16^k with
+    x = w8192^j (the data-availability checks of fk20_multi.py:154-165 use
+    x = w8192^rbo(pos) for proof pos of the bit-reversed list).  Valid proofs
+    pass; a wrong value, a proof of another coset and another polynomial's
+    commitment fail.  A second call with l = 4 checks a proof built from the
+    KZG definitions, against the restatement's verdicts."""
+    import torch
+    n, m, l = 4096, 512, 16
+    tau, setup, xext = fk20_setup_data(n)
+    t = O.limbs_to_int(tau)
+    polys = O.seeded_fr(9200, 2 * n).reshape(2, n, 4)
+    c = engine.Context(0, 8)
+    c.load_xext_fft(n, engine.to_device(xext))
+    c.load_commit(n, engine.to_device(setup[:n]), 8)
+    dpolys = engine.to_device(polys)
+    h = engine.empty((1, m, 18))
+    c.poly2h_fft(h, dpolys[0:1], 1, n)
+    com = engine.empty((2, 18))
+    c.commit(com, dpolys, 2, n)
+    hh, cc = engine.to_host(h)[0], engine.to_host(com)
+    f = [O.limbs_to_int(v) for v in polys[0]]
+
+    def evalf(z):
+        acc = 0
+        for coef in reversed(f):
+            acc = (acc * z + coef) % O.R
+        return acc
+
+    w8192, w16 = O.root_of_unity(2 * n), O.root_of_unity(16)
+    js = [0, 1, 77, 255, 256, 511]
+    xs = [pow(w8192, j, O.R) for j in js]
+    yss = [[evalf(x * pow(w16, k, O.R) % O.R) for k in range(l)] for x in xs]
+    bad_ys = list(yss[0])
+    bad_ys[3] = (bad_ys[3] + 1) % O.R
+    cases = [(cc[0], hh[j], x, ys) for j, x, ys in zip(js, xs, yss)]
+    cases += [(cc[0], hh[js[0]], xs[0], bad_ys),  # a wrong value
+              (cc[0], hh[js[1] + 1], xs[1], yss[1]),  # the proof of another coset
+              (cc[1], hh[js[2]], xs[2], yss[2])]  # another polynomial's commitment
+    expect = [1] * len(js) + [0, 0, 0]
+    G2 = PP.g2_generator()
+    setup_g2 = engine.to_device(g2_to_array([PP.g2mul(pow(t, k, O.R), G2) for k in range(l + 1)]))
+    dev = lambda a: engine.to_device(np.ascontiguousarray(a))
+    C = dev(np.stack([q[0] for q in cases]))
+    Pf = dev(np.stack([q[1] for q in cases]))
+    X = dev(np.stack([O.int_to_limbs(q[2], 4) for q in cases]))
+    Y = dev(np.stack([np.stack([O.int_to_limbs(v, 4) for v in q[3]]) for q in cases]))
+    ok = torch.zeros(len(cases), dtype=torch.uint8, device="cuda")
+    c.check_proof_multi(ok, C, Pf, X, Y, l, setup_g2, len(cases))
+    assert ok.cpu().numpy().tolist() == expect
+
+    # l = 4, a proof from the definitions (same tau as the context's tables)
+    small = kzg_multi_case(l=4, tau=t)
+    bad = list(small["ys"])
+    bad[1] = (bad[1] + 1) % O.R
+    verdicts = [PP.check_proof_multi(small["commitment"], small["proof"], small["x"], ys, small["setup_g1"],
+                                     small["setup_g2"]) for ys in (small["ys"], bad)]
+    assert verdicts == [True, False]
+    C4 = dev(g1_to_array([small["commitment"]] * 2))
+    P4 = dev(g1_to_array([small["proof"]] * 2))
+    X4 = dev(np.stack([O.int_to_limbs(small["x"], 4)] * 2))
+    Y4 = dev(np.stack([np.stack([O.int_to_limbs(v, 4) for v in ys]) for ys in (small["ys"], bad)]))
+    ok4 = torch.zeros(2, dtype=torch.uint8, device="cuda")
+    c.check_proof_multi(ok4, C4, P4, X4, Y4, 4, dev(g2_to_array(small["setup_g2"])), 2)
+    assert [bool(v) for v in ok4.cpu().numpy()] == verdicts
     c.close()

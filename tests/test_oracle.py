@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from conftest import kzg_multi_case
 import fk20_py as PY
 
 P, R = O.P, O.R
@@ -244,3 +245,15 @@ def test_pairing_restatement_is_bilinear():
     assert PP.pairing(g1mul(a), PP.g2mul(b, G2)) == PP.f12pow(e, a * b % O.R)
     assert PP.pairing_check(g1mul(a), PP.g2mul(b, G2), g1mul(a * b), G2)
     assert not PP.pairing_check(g1mul(a), PP.g2mul(b, G2), g1mul(a * b + 1), G2)
+
+
+def test_check_proof_multi_restatement():
+    """oracle/pairing_py.check_proof_multi (FK20Py/kzg_proofs.py:207-232)
+    accepts a proof built from the KZG definitions and rejects a wrong value."""
+    import pairing_py as PP
+    c = kzg_multi_case()
+    args = (c["setup_g1"], c["setup_g2"])
+    assert PP.check_proof_multi(c["commitment"], c["proof"], c["x"], c["ys"], *args)
+    bad = list(c["ys"])
+    bad[1] = (bad[1] + 1) % O.R
+    assert not PP.check_proof_multi(c["commitment"], c["proof"], c["x"], bad, *args)
