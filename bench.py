@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--serve-latency-rows", type=int, default=0,
                     help="latency-mode packs while at most this many requests wait (0: max rows)")
     ap.add_argument("--autotune", action="store_true", help="autotune the context before timing (batch, ragged)")
+    ap.add_argument("--msm-threads", type=int, default=0, help="MSM block size (64, 128, 256; 0 = the context's)")
     ap.add_argument("--tune-max-table-bytes", type=int, default=0,
                     help="table memory budget of the autotuner (0 = what the free device memory allows)")
     return ap.parse_args()
@@ -311,6 +312,8 @@ def run_ours(args, ws, rank, dev):
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     tune = None
+    if args.msm_threads:
+        ctx.set(E.FK20_OPT_MSM_THREADS, args.msm_threads)
     if args.autotune:  # window within the memory budget, MSM block size, FFT grid, fused vs staged
         t1 = time.time()
         tune = ctx.autotune(n, rows=min(rows, 512), max_table_bytes=args.tune_max_table_bytes)

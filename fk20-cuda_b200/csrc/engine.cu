@@ -261,7 +261,7 @@ struct Workspace {
 // Per-launch profiling: CUDA events on the launching stream around every
 // pipeline kernel, with the algorithmic work of that launch (in 32x32->64-bit
 // limb products: Fp product M_p = 300, Fr product M_r = 136, RCB addition
-// 12 M_p, mixed addition 11 M_p, doubling 8 M_p).
+// 12 M_p, XYZZ mixed addition 10 M_p, doubling 8 M_p).
 struct Profiler {
     bool on = false;
     struct Rec {
@@ -357,7 +357,9 @@ struct DeviceGuard {  // make ctx->device current for the duration of a call
 };
 
 // ---- algorithmic work model (limb products) ----------------------------------
-constexpr double MP = 300.0, MR = 136.0, ADD_P = 12 * MP, MADD_P = 11 * MP, DBL_P = 8 * MP;
+// Fp products per operation: complete projective addition 12, doubling 8; the
+// MSM's mixed addition into an XYZZ accumulator 10 (8 M + 2 S)
+constexpr double MP = 300.0, MR = 136.0, ADD_P = 12 * MP, MADD_P = 10 * MP, DBL_P = 8 * MP;
 
 double prog_products(int idx) {
     const HostConsts &hc = host_consts();

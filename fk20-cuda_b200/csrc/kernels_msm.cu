@@ -5,9 +5,13 @@
 // has a table of its signed-digit multiples: entry (w, e) = (e+1) 2^(cb w) X,
 // e < 2^(cb-1), affine Montgomery (built by kernels_tables.cu).  A 255-bit
 // scalar is recoded on the fly into ceil(255/cb) signed digits in
-// [-2^(cb-1), 2^(cb-1)] and each nonzero digit costs one mixed addition
-// (RCB Algorithm 8) of a gathered 96-byte entry: no doublings at all, against
-// ~255 doublings + ~128 additions per term in the reference's g1p_mul loop.
+// [-2^(cb-1), 2^(cb-1)] and each nonzero digit costs one mixed addition of a
+// gathered 96-byte entry: no doublings at all, against ~255 doublings + ~128
+// additions per term in the reference's g1p_mul loop.  The accumulator is in
+// XYZZ coordinates (x = X/ZZ, y = Y/ZZZ), whose mixed addition takes 8 M + 2 S
+// (the complete projective one 11 M); its exceptional cases -- accumulator at
+// infinity, equal or opposite points -- are tested and handled, so every sum
+// is exact.  The result goes back to homogeneous projective coordinates.
 #if defined(FK_MSM_OUTLINE) && FK_MSM_OUTLINE
 #define FK_FP_MUL_OUTLINE 1
 #endif
@@ -29,11 +33,89 @@ namespace fk {
 
 cudaError_t upload_consts_msm() { return upload_module_consts(); }
 
+// XYZZ point: x = X / ZZ, y = Y / ZZZ (ZZ^3 = ZZZ^2); ZZ = 0 is infinity
+struct G1Z {
+    Fp x, y, zz, zzz;
+};
+FK_D void g1z_set_inf(G1Z &a) {
+    f_set_one(a.x);
+    f_set_one(a.y);
+    f_set_zero(a.zz);
+    f_set_zero(a.zzz);
+}
+// a = 2 (qx, qy), affine q not infinity (y != 0 in the prime-order group):
+// U = 2y, V = U^2, W = U V, S = x V, M = 3 x^2, X = M^2 - 2S,
+// Y = M (S - X) - W y, ZZ = V, ZZZ = W
+FK_D void g1z_dbl_affine(G1Z &a, const Fp &qx, const Fp &qy) {
+    Fp u, v, w, sv, m, t;
+    f_add(u, qy, qy);
+    fp_sqr(v, u);
+    fp_mul(w, u, v);
+    fp_mul(sv, qx, v);
+    fp_sqr(m, qx);
+    f_add(t, m, m);
+    f_add(m, t, m);
+    fp_sqr(t, m);
+    f_sub(t, t, sv);
+    f_sub(a.x, t, sv);
+    f_sub(t, sv, a.x);
+    fp_mul(t, m, t);
+    fp_mul(u, w, qy);
+    f_sub(a.y, t, u);
+    a.zz = v;
+    a.zzz = w;
+}
+// a += (qx, qy), affine q not infinity (madd-2008-s: U2 = qx ZZ, S2 = qy ZZZ,
+// P = U2 - X, R = S2 - Y, X3 = R^2 - P^3 - 2 X P^2, Y3 = R (X P^2 - X3) - Y P^3,
+// ZZ3 = ZZ P^2, ZZZ3 = ZZZ P^3)
+FK_D void g1z_madd(G1Z &a, const Fp &qx, const Fp &qy) {
+    if (f_is_zero(a.zz)) {
+        a.x = qx;
+        a.y = qy;
+        f_set_one(a.zz);
+        f_set_one(a.zzz);
+        return;
+    }
+    Fp u2, s2, p, r, pp, ppp, q, t;
+    fp_mul(u2, qx, a.zz);
+    fp_mul(s2, qy, a.zzz);
+    f_sub(p, u2, a.x);
+    f_sub(r, s2, a.y);
+    if (f_is_zero(p)) {
+        if (f_is_zero(r)) g1z_dbl_affine(a, qx, qy);  // a = q
+        else g1z_set_inf(a);                          // a = -q
+        return;
+    }
+    fp_sqr(pp, p);
+    fp_mul(ppp, p, pp);
+    fp_mul(q, a.x, pp);
+    fp_sqr(t, r);
+    f_sub(t, t, ppp);
+    f_sub(t, t, q);
+    f_sub(a.x, t, q);
+    f_sub(t, q, a.x);
+    fp_mul(t, r, t);
+    fp_mul(s2, a.y, ppp);
+    f_sub(a.y, t, s2);
+    fp_mul(a.zz, a.zz, pp);
+    fp_mul(a.zzz, a.zzz, ppp);
+}
+// homogeneous projective (X ZZZ, Y ZZ, ZZ ZZZ); infinity as (0, 1, 0)
+FK_D void g1z_to_proj(G1P &r, const G1Z &a) {
+    if (f_is_zero(a.zz)) {
+        g1_set_inf(r);
+        return;
+    }
+    fp_mul(r.x, a.x, a.zzz);
+    fp_mul(r.y, a.y, a.zz);
+    fp_mul(r.z, a.zz, a.zzz);
+}
+
 // acc += s * X for one base X, whose table `tb` holds (e+1) 2^(cb w) X for
 // window w and e < 2^(cb-1): the 255-bit scalar s (9 words, s[8] = 0) is
 // recoded into W signed digits in [-2^(cb-1), 2^(cb-1)] on the fly and every
 // nonzero digit costs one mixed addition of a gathered 96-byte entry.
-FK_D void msm_add_scalar(G1P &acc, const uint32_t s[9], const uint4 *__restrict__ tb, int W, int cb) {
+FK_D void msm_add_scalar(G1Z &acc, const uint32_t s[9], const uint4 *__restrict__ tb, int W, int cb) {
     const int E = 1 << (cb - 1);
     const uint32_t mask = (1u << cb) - 1u;
     int carry = 0;
@@ -59,7 +141,7 @@ FK_D void msm_add_scalar(G1P &acc, const uint32_t s[9], const uint4 *__restrict_
             // an entry (0, 0) encodes a base at infinity (not on the curve)
             if (!(f_is_zero(x) && f_is_zero(y))) {
                 if (d < 0) f_neg(y, y);
-                g1_madd(acc, acc, x, y);
+                g1z_madd(acc, x, y);
             }
         }
     }
@@ -81,8 +163,8 @@ __global__ void __launch_bounds__(MSM_MAX_THREADS, FK_MSM_MINB) k_msm(const __gr
     const int row = g * 32 + lane;
     const bool live = row < a.rows;
     const int E = 1 << (a.cb - 1);
-    G1P acc;
-    g1_set_inf(acc);
+    G1Z accz;
+    g1z_set_inf(accz);
     for (int i = 0; i < L_COLS; i++) {
         uint32_t s[9];
         const uint4 *src = a.S + ((((size_t)g * m + c) * L_COLS + i) * SCAL_Q) * 32 + lane;
@@ -95,8 +177,10 @@ __global__ void __launch_bounds__(MSM_MAX_THREADS, FK_MSM_MINB) k_msm(const __gr
             for (int k = 0; k < 9; k++) s[k] = 0;
         }
         const uint4 *tb = a.table + ((size_t)(i * m + c) * a.W) * E * 6;
-        msm_add_scalar(acc, s, tb, a.W, a.cb);
+        msm_add_scalar(accz, s, tb, a.W, a.cb);
     }
+    G1P acc;
+    g1z_to_proj(acc, accz);
     if (args.times_m) {
         for (int t = 0; t < a.log_m; t++) g1_dbl(acc, acc);
     }
@@ -120,8 +204,8 @@ __global__ void __launch_bounds__(128) k_commit_partial(uint4 *__restrict__ part
     const int row = g * 32 + lane;
     const bool live = row < rows;
     const int E = 1 << (cb - 1);
-    G1P acc;
-    g1_set_inf(acc);
+    G1Z accz;
+    g1z_set_inf(accz);
     for (int i = c * COMMIT_CHUNK; i < (c + 1) * COMMIT_CHUNK; i++) {
         uint32_t s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         if (live) {
@@ -130,8 +214,10 @@ __global__ void __launch_bounds__(128) k_commit_partial(uint4 *__restrict__ part
 #pragma unroll
             for (int k = 0; k < 8; k++) s[k] = f.w[k];
         }
-        msm_add_scalar(acc, s, table + (size_t)i * W * E * 6, W, cb);
+        msm_add_scalar(accz, s, table + (size_t)i * W * E * 6, W, cb);
     }
+    G1P acc;
+    g1z_to_proj(acc, accz);
     tile_store(part + tile_index(g, chunks, c), lane, acc);
 }
 
