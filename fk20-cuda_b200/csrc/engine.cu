@@ -364,7 +364,7 @@ constexpr double MP = 300.0, MR = 136.0, ADD_P = 12 * MP, MADD_P = 10 * MP, DBL_
 double prog_products(int idx) {
     const HostConsts &hc = host_consts();
     if (hc.prog[idx][0] & 0x300u) return 0.0;
-    return hc.prog_dbl[idx] * DBL_P + hc.prog_add[idx] * ADD_P + MP;  // + phi(P)
+    return hc.prog_dbl[idx] * DBL_P + hc.prog_add[idx] * ADD_P + PROG_SLOTS * MP;  // + beta x of P, 3P, 5P, 7P
 }
 
 // one stage over `rows` rows: kind 0 DIF inverse, 1 DIT forward

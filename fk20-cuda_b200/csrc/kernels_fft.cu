@@ -35,7 +35,7 @@ cudaError_t upload_consts_fft() { return upload_module_consts(); }
 // kind 1: DIT with forward twiddles (bit-reversed in, natural out).
 template <int KIND>
 __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__restrict__ D, int G, int log_m, int s) {
-    __shared__ uint32_t slots[36 * PROG_SLOTS][FFT_THREADS];
+    __shared__ uint32_t slots[PROG_SLOT_WORDS][FFT_THREADS];
     const int m = 1 << log_m;
     const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -55,8 +55,7 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_stage(uint4 *__
     const int i0 = ((b / half) * 2 * half) + j, i1 = i0 + half;
     uint4 *p0 = D + tile_index(g, m, i0);
     uint4 *p1 = D + tile_index(g, m, i1);
-    const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS}, {&slots[36][threadIdx.x], FFT_THREADS},
-                                           {&slots[72][threadIdx.x], FFT_THREADS}, {&slots[108][threadIdx.x], FFT_THREADS}};
+    const ProgSlots slot{&slots[0][threadIdx.x], FFT_THREADS};
     // Points pass through the shared-memory slots so that only the accumulator
     // of the current point operation is held in registers.
     G1P acc;
@@ -152,12 +151,11 @@ FK_D bool wait_ready(const unsigned *ra, const unsigned *rb, unsigned need, int 
 }
 
 __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_fused(const __grid_constant__ FusedPlan P) {
-    __shared__ uint32_t slots[36 * PROG_SLOTS][FFT_THREADS];
+    __shared__ uint32_t slots[PROG_SLOT_WORDS][FFT_THREADS];
     const int lane = threadIdx.x & 31;
     const unsigned total = P.blk.start[P.blk.nblk];
     const unsigned base = P.epoch * 64u;
-    const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS}, {&slots[36][threadIdx.x], FFT_THREADS},
-                                           {&slots[72][threadIdx.x], FFT_THREADS}, {&slots[108][threadIdx.x], FFT_THREADS}};
+    const ProgSlots slot{&slots[0][threadIdx.x], FFT_THREADS};
     for (;;) {
         unsigned task = 0;
         if (lane == 0) task = atomicAdd(P.next, 1u);
@@ -236,7 +234,9 @@ void launch_g1_fused(const FusedPlan &p, cudaStream_t st) {
 // (2q, 2q+1) -> both = a + b, optionally times 2^-log_m
 template <bool SCALE>
 __global__ void __launch_bounds__(FFT_THREADS) k_g1_middle(uint4 *__restrict__ D, int G, int log_m) {
-    __shared__ uint32_t slots[SCALE ? 36 * PROG_SLOTS : 1][FFT_THREADS];
+    // the program scratch (SCALE), whose point 1 also holds b for the sum;
+    // without SCALE one point of scratch
+    __shared__ uint32_t slots[SCALE ? PROG_SLOT_WORDS : 36][FFT_THREADS];
     const int m = 1 << log_m;
     const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -244,17 +244,13 @@ __global__ void __launch_bounds__(FFT_THREADS) k_g1_middle(uint4 *__restrict__ D
     if (q >= (m >> 1)) return;
     uint4 *p0 = D + tile_index(g, m, 2 * q);
     uint4 *p1 = D + tile_index(g, m, 2 * q + 1);
-    __shared__ uint32_t vs[36][FFT_THREADS];
-    const StridedPoint sv{&vs[0][threadIdx.x], FFT_THREADS};
+    const StridedPoint sv{&slots[SCALE ? 36 : 0][threadIdx.x], FFT_THREADS};
     G1P x;
     tile_to_slot(sv, p1, lane);
     tile_load(x, p0, lane);
     g1_add_q(x, x, sv, false);
     if (SCALE) {
-        const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS},
-                                               {&slots[SCALE ? 36 : 0][threadIdx.x], FFT_THREADS},
-                                               {&slots[SCALE ? 72 : 0][threadIdx.x], FFT_THREADS},
-                                               {&slots[SCALE ? 108 : 0][threadIdx.x], FFT_THREADS}};
+        const ProgSlots slot{&slots[0][threadIdx.x], FFT_THREADS};
         slot[0].put(x);
         g1_mul_prog(x, slot, c_prog[512 + log_m]);
     }
@@ -264,15 +260,14 @@ __global__ void __launch_bounds__(FFT_THREADS) k_g1_middle(uint4 *__restrict__ D
 
 // every point of the tiles times program `prog`
 __global__ void __launch_bounds__(FFT_THREADS) k_g1_scale(uint4 *__restrict__ D, int G, int log_m, int prog) {
-    __shared__ uint32_t slots[36 * PROG_SLOTS][FFT_THREADS];
+    __shared__ uint32_t slots[PROG_SLOT_WORDS][FFT_THREADS];
     const int m = 1 << log_m;
     const int warp = blockIdx.x * (FFT_THREADS / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     const int g = warp % G, i = warp / G;
     if (i >= m) return;
     uint4 *p = D + tile_index(g, m, i);
-    const StridedPoint slot[PROG_SLOTS] = {{&slots[0][threadIdx.x], FFT_THREADS}, {&slots[36][threadIdx.x], FFT_THREADS},
-                                           {&slots[72][threadIdx.x], FFT_THREADS}, {&slots[108][threadIdx.x], FFT_THREADS}};
+    const ProgSlots slot{&slots[0][threadIdx.x], FFT_THREADS};
     G1P u;
     tile_to_slot(slot[0], p, lane);
     g1_mul_prog(u, slot, c_prog[prog]);

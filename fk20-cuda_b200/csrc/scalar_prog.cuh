@@ -7,19 +7,19 @@
 // with the GLV endomorphism of BLS12-381 G1: k = k1 + k2*lambda (mod r) with
 // lambda = z^2 - 1 ~ 2^128, r = lambda^2 + lambda + 1, so k2 = k div lambda and
 // k1 = k mod lambda are both < 2^128, and [k]P = [k1]P + [k2]phi(P) with
-// phi(x, y) = (beta x, y).  k1 and k2 are recoded in width-3 NAF (digits 0,
-// +-1, +-3; nonzero digits at least 3 apart) and processed jointly over the
-// precomputed P, 3P, phi(P), phi(3P): ~124 doublings and ~62 additions
-// instead of ~254 and ~128.  Of k and r - k the cheaper one is encoded (and
-// the result negated).  The result equals [k]P for every P in the order-r
-// subgroup -- all FK20 data.
+// phi(x, y) = (beta x, y).  k1 and k2 are recoded in width-4 NAF (digits 0,
+// +-1, +-3, +-5, +-7; nonzero digits at least 4 apart) and processed jointly
+// over the precomputed P, 3P, 5P, 7P and their images under phi, which differ
+// only in x (beta x): ~124 doublings and ~49 additions instead of ~254 and
+// ~128.  Of k and r - k the cheaper one is encoded (and the result negated).
+// The result equals [k]P for every P in the order-r subgroup -- all FK20 data.
 //
 // Program layout (PROG_WORDS uint32 words):
 //   word 0      : bits 0-7 top digit position, bit 8 = scalar is 0,
 //                 bit 9 = scalar is +-1, bit 10 = negate the result
 //   words 1..34 : one byte per digit position p (word 1 + p/4, byte p%4):
-//                 bits 0-2 the k1 digit, bits 4-6 the k2 digit, each coded as
-//                 bit0 nonzero, bit1 negative, bit2 magnitude 3 (else 1)
+//                 bits 0-3 the k1 digit, bits 4-7 the k2 digit, each coded as
+//                 bit0 nonzero, bit1 negative, bits 2-3 (|digit| - 1) / 2
 // A warp runs one program for 32 independent points, so every branch in the
 // executor is warp-uniform.
 #pragma once
@@ -29,35 +29,74 @@ namespace fk {
 
 constexpr int PROG_POSITIONS = 136;
 constexpr int PROG_WORDS = 1 + PROG_POSITIONS / 4;
-constexpr int PROG_SLOTS = 4;  // P, 3P, phi(P), phi(3P)
+constexpr int PROG_SLOTS = 4;                         // P, 3P, 5P, 7P
+constexpr int PROG_SLOT_WORDS = 36 * PROG_SLOTS + 12 * PROG_SLOTS;  // + beta x of each
+
+// The executor's scratch: for each thread PROG_SLOT_WORDS 32-bit words at
+// base[0], base[stride], ...: point i (x, y, z) at word 36 i, beta x_i at
+// word 144 + 12 i.  Addresses are formed when used, so the scratch costs one
+// pointer of registers.
+struct ProgSlots {
+    uint32_t *base;
+    int stride;
+    FK_HD StridedPoint pt(int i) const { return StridedPoint{base + 36 * i * stride, stride}; }
+    FK_HD StridedPoint operator[](int i) const { return pt(i); }
+    FK_HD uint32_t *bx(int i) const { return base + (36 * PROG_SLOTS + 12 * i) * stride; }
+};
+
+// Q = point i of the slots or its image phi(Q) = (beta x, y, z): x read from
+// one of two places, y and z shared
+struct SlotQ {
+    const uint32_t *x, *yz;
+    int stride;
+    FK_HD void get(int c, Fp &f) const {
+        const uint32_t *src = c == 0 ? x : yz + 12 * (c - 1) * stride;
+#pragma unroll
+        for (int k = 0; k < 12; k++) f.w[k] = src[k * stride];
+    }
+    FK_HD void load(G1P &p) const {
+        get(0, p.x);
+        get(1, p.y);
+        get(2, p.z);
+    }
+};
 
 // acc = [k] P for the program of k (P in the prime-order subgroup).  P is
-// read from slot[0]; slots 1..3 receive 3P, phi(P), phi(3P).  Only the
+// read from point 0 of the slots; points 1..3 receive 3P, 5P, 7P and the
+// beta x rows the x of phi(P), phi(3P), phi(5P), phi(7P).  Only the
 // accumulator lives in registers.
 template <class ProgPtr>
-FK_HD void g1_mul_prog(G1P &acc, const StridedPoint *slot, ProgPtr prog) {
+FK_HD void g1_mul_prog(G1P &acc, const ProgSlots &slot, ProgPtr prog) {
     const uint32_t hdr = prog[0];
     if (hdr & 0x100u) { g1_set_inf(acc); return; }
     const bool negate = (hdr & 0x400u) != 0;
     if (hdr & 0x200u) {
-        slot[0].load(acc);
+        slot.pt(0).load(acc);
         if (negate) f_neg(acc.y, acc.y);
         return;
     }
     {
-        Fp beta;
+        // 2P parked in point 3; 3P = P + 2P, 5P = 3P + 2P, 7P = 5P + 2P
+        slot.pt(0).load(acc);
+        g1_dbl(acc, acc);
+        slot.pt(3).put(acc);
+        slot.pt(0).load(acc);
+#pragma unroll 1
+        for (int i = 1; i < PROG_SLOTS; i++) {
+            g1_add_q(acc, acc, slot.pt(3), false);
+            slot.pt(i).put(acc);
+        }
+        Fp beta, x;
 #pragma unroll
         for (int i = 0; i < 12; i++) beta.w[i] = beta_mont(i);
-        // 3P = 2P + P, then phi(P), phi(3P)
-        slot[0].load(acc);
-        g1_dbl(acc, acc);
-        g1_add_q(acc, acc, slot[0], false);
-        slot[1].put(acc);
-        fp_mul(acc.x, acc.x, beta);
-        slot[3].put(acc);
-        slot[0].load(acc);
-        fp_mul(acc.x, acc.x, beta);
-        slot[2].put(acc);
+#pragma unroll 1
+        for (int i = 0; i < PROG_SLOTS; i++) {
+            slot.pt(i).get(0, x);
+            fp_mul(x, x, beta);
+            uint32_t *dst = slot.bx(i);
+#pragma unroll
+            for (int k = 0; k < 12; k++) dst[k * slot.stride] = x.w[k];
+        }
     }
     const int top = (int)(hdr & 0xffu);
     bool started = false;
@@ -65,9 +104,11 @@ FK_HD void g1_mul_prog(G1P &acc, const StridedPoint *slot, ProgPtr prog) {
         if (started) g1_dbl(acc, acc);
         const uint32_t byte = (prog[1 + (pos >> 2)] >> ((pos & 3) * 8)) & 0xffu;
         for (int h = 0; h < 2; h++) {
-            const uint32_t d = (byte >> (4 * h)) & 7u;
+            const uint32_t d = (byte >> (4 * h)) & 15u;
             if (d & 1u) {
-                const StridedPoint q = slot[2 * h + ((d >> 2) & 1u)];
+                const int i = (int)(d >> 2);
+                const uint32_t *pt = slot.base + 36 * i * slot.stride;
+                const SlotQ q{h ? slot.bx(i) : pt, pt + 12 * slot.stride, slot.stride};
                 if (started) {
                     g1_add_q(acc, acc, q, (d & 2u) != 0);
                 } else {
@@ -85,9 +126,9 @@ FK_HD void g1_mul_prog(G1P &acc, const StridedPoint *slot, ProgPtr prog) {
 // local scratch array stands in for the slots
 template <class ProgPtr>
 FK_HD void g1_mul_prog(G1P &R, const G1P &P, ProgPtr prog) {
-    uint32_t mem[36 * PROG_SLOTS];
-    const StridedPoint slot[PROG_SLOTS] = {{mem, 1}, {mem + 36, 1}, {mem + 72, 1}, {mem + 108, 1}};
-    slot[0].put(P);
+    uint32_t mem[PROG_SLOT_WORDS];
+    const ProgSlots slot{mem, 1};
+    slot.pt(0).put(P);
     g1_mul_prog(R, slot, prog);
 }
 
@@ -121,15 +162,15 @@ inline void divmod256(uint64_t q[4], uint64_t rem[4], const uint64_t a[4], const
     for (int i = 0; i < 4; i++) rem[i] = r[i];
 }
 
-// width-3 NAF digits (0, +-1, +-3) of k < 2^128 into d[0..PROG_POSITIONS);
-// returns the top position or -1
-inline int wnaf3(int8_t *d, unsigned __int128 k) {
+// width-4 NAF digits (0, +-1, +-3, +-5, +-7) of k < 2^128 into
+// d[0..PROG_POSITIONS); returns the top position or -1
+inline int wnaf4(int8_t *d, unsigned __int128 k) {
     int top = -1;
     for (int i = 0; i < PROG_POSITIONS; i++) d[i] = 0;
     for (int i = 0; k != 0; i++) {
         if (k & 1) {
-            int v = (int)(k & 7);
-            if (v >= 4) v -= 8;
+            int v = (int)(k & 15);
+            if (v >= 8) v -= 16;
             d[i] = (int8_t)v;
             if (v > 0) k -= (unsigned)v; else k += (unsigned)(-v);
             top = i;
@@ -141,7 +182,8 @@ inline int wnaf3(int8_t *d, unsigned __int128 k) {
 
 inline uint32_t digit_code(int v) {
     if (v == 0) return 0;
-    return 1u | (v < 0 ? 2u : 0u) | ((v == 3 || v == -3) ? 4u : 0u);
+    const int m = v < 0 ? -v : v;
+    return 1u | (v < 0 ? 2u : 0u) | ((uint32_t)((m - 1) / 2) << 2);
 }
 
 // program for a standard-form scalar k < r (4 x 64-bit words), no sign choice
@@ -157,7 +199,7 @@ inline void make_program_raw(uint32_t prog[PROG_WORDS], const uint64_t k[4]) {
     unsigned __int128 k1 = ((unsigned __int128)rem[1] << 64) | rem[0];
     unsigned __int128 k2 = ((unsigned __int128)q[1] << 64) | q[0];
     int8_t d1[PROG_POSITIONS], d2[PROG_POSITIONS];
-    int t1 = wnaf3(d1, k1), t2 = wnaf3(d2, k2);
+    int t1 = wnaf4(d1, k1), t2 = wnaf4(d2, k2);
     int top = t1 > t2 ? t1 : t2;
     prog[0] = (uint32_t)top;
     for (int p = 0; p <= top; p++) {
@@ -166,15 +208,15 @@ inline void make_program_raw(uint32_t prog[PROG_WORDS], const uint64_t k[4]) {
     }
 }
 
-// algorithmic cost of a program in doublings and additions (the 3P
-// precompute included: 1 doubling + 1 addition; the two phi products are not)
+// algorithmic cost of a program in doublings and additions (the 3P, 5P, 7P
+// precompute included: 1 doubling + 3 additions; the four phi products are not)
 inline void program_cost(const uint32_t prog[PROG_WORDS], int *dbl, int *add) {
     *dbl = *add = 0;
     if (prog[0] & 0x300u) return;
     int top = (int)(prog[0] & 0xff);
     bool started = false;
     *dbl = 1;
-    *add = 1;
+    *add = PROG_SLOTS - 1;
     for (int p = top; p >= 0; p--) {
         if (started) (*dbl)++;
         const uint32_t byte = (prog[1 + (p >> 2)] >> ((p & 3) * 8)) & 0xff;
