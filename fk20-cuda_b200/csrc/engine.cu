@@ -1259,8 +1259,9 @@ int fk20_ctx_commit(fk20_ctx *ctx, g1p_t *commitment, const fr_t *polynomial, un
     DeviceGuard dg(ctx->device);
     if (!ctx->commit.n || (int)n > ctx->commit.n) return FK20_ENOSETUP;
     const int G = (int)((rows + 31) / 32);
-    CKR(ctx->commit.part.reserve(tile_bytes(G, (int)(n / COMMIT_CHUNK))));
-    const double prod = (double)rows * n * ctx->commit.W * MADD_P + (double)rows * (n / COMMIT_CHUNK) * ADD_P;
+    const int parts = commit_parts((int)rows, (int)n);
+    CKR(ctx->commit.part.reserve(tile_bytes(G, parts)));
+    const double prod = (double)rows * n * ctx->commit.W * MADD_P + (double)rows * parts * ADD_P;
     ctx->prof.begin(FK20_K_MSM, prod, S_(stream));
     launch_commit((uint64_t *)commitment, (uint4 *)ctx->commit.part.p, (const uint64_t *)polynomial,
                   (const uint4 *)ctx->commit.table.p, (int)rows, (int)n, ctx->commit.W, ctx->commit.cb, S_(stream));
@@ -1459,7 +1460,7 @@ int fk20_ctx_check_proof_multi(fk20_ctx *ctx, uint8_t *ok, const g1p_t *commitme
     const size_t poly_b = (size_t)count * COMMIT_CHUNK * sizeof(fr_t), xl_b = (size_t)count * sizeof(fr_t),
                  pt_b = (size_t)count * sizeof(g1p_t);
     CKR(ctx->verify.reserve(poly_b + xl_b + 3 * pt_b));
-    CKR(ctx->commit.part.reserve(tile_bytes(G, 1)));
+    CKR(ctx->commit.part.reserve(tile_bytes(G, commit_parts((int)count, (int)COMMIT_CHUNK))));
     char *base = (char *)ctx->verify.p;
     uint64_t *poly = (uint64_t *)base, *xl = (uint64_t *)(base + poly_b);
     uint64_t *I = (uint64_t *)(base + poly_b + xl_b), *T = I + 18 * (size_t)count, *A = T + 18 * (size_t)count;

@@ -15,6 +15,8 @@
 #if defined(FK_MSM_OUTLINE) && FK_MSM_OUTLINE
 #define FK_FP_MUL_OUTLINE 1
 #endif
+#include <algorithm>
+
 #include "consts.cuh"
 #include "launch.h"
 #include "layout.cuh"
@@ -190,23 +192,26 @@ __global__ void __launch_bounds__(MSM_MAX_THREADS, FK_MSM_MINB) k_msm(const __gr
 // ---------------------------------------------------------------- KZG commitments
 // commitment[row] = sum_i poly[row][i] * s_i over fixed-base tables of the
 // setup points s_i (commit_to_poly, FK20Py/kzg_proofs.py:159-163).  Pass 1:
-// warp (g, chunk) sums the COMMIT_CHUNK bases of its chunk for 32 rows into a
-// partial-sum tile; pass 2: one thread per row adds its chunks' partials.
+// warp (g, p) sums bases [p n / P, (p+1) n / P) for the 32 rows of group g
+// into a partial-sum tile, P = commit_parts(rows, n) warps per group, chosen
+// so that pass 1 is one wave of resident warps (whole warps of fixed chunks
+// left a second, mostly idle wave); pass 2: one thread per row adds its P
+// partials.
 __global__ void __launch_bounds__(128) k_commit_partial(uint4 *__restrict__ part, const uint64_t *__restrict__ poly,
                                                         const uint4 *__restrict__ table, int rows, int n, int W,
-                                                        int cb) {
-    const int chunks = n / COMMIT_CHUNK;
+                                                        int cb, int P) {
     const int G = (rows + 31) / 32;
     const unsigned warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (warp >= (unsigned)G * chunks) return;
+    if (warp >= (unsigned)G * P) return;
     const int lane = threadIdx.x & 31;
     const int g = (int)(warp % (unsigned)G), c = (int)(warp / (unsigned)G);
     const int row = g * 32 + lane;
     const bool live = row < rows;
     const int E = 1 << (cb - 1);
+    const int i0 = (int)((long long)c * n / P), i1 = (int)((long long)(c + 1) * n / P);
     G1Z accz;
     g1z_set_inf(accz);
-    for (int i = c * COMMIT_CHUNK; i < (c + 1) * COMMIT_CHUNK; i++) {
+    for (int i = i0; i < i1; i++) {
         uint32_t s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         if (live) {
             Fr f;
@@ -218,27 +223,46 @@ __global__ void __launch_bounds__(128) k_commit_partial(uint4 *__restrict__ part
     }
     G1P acc;
     g1z_to_proj(acc, accz);
-    tile_store(part + tile_index(g, chunks, c), lane, acc);
+    tile_store(part + tile_index(g, P, c), lane, acc);
 }
 
-__global__ void k_commit_reduce(uint64_t *__restrict__ out, const uint4 *__restrict__ part, int rows, int chunks) {
+__global__ void k_commit_reduce(uint64_t *__restrict__ out, const uint4 *__restrict__ part, int rows, int P) {
     for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
         const int g = row >> 5, lane = row & 31;
         G1P acc, q;
-        tile_load(acc, part + tile_index(g, chunks, 0), lane);
-        for (int c = 1; c < chunks; c++) {
-            tile_load(q, part + tile_index(g, chunks, c), lane);
+        tile_load(acc, part + tile_index(g, P, 0), lane);
+        for (int c = 1; c < P; c++) {
+            tile_load(q, part + tile_index(g, P, c), lane);
             g1_add(acc, acc, q);
         }
         g1p_to_ref(out + 18 * (size_t)row, acc);
     }
 }
 
+// pass-1 warps per group of 32 rows: one wave of the warps the device holds
+// at once, at least one, at most one per base
+int commit_parts(int rows, int n) {
+    static int resident = 0;  // warps of k_commit_partial resident on the device
+    if (!resident) {
+        int dev = 0, sms = 1, bps = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_commit_partial, 128, 0) != cudaSuccess || bps < 1) {
+            cudaGetLastError();
+            bps = 1;
+        }
+        resident = sms * bps * 4;
+    }
+    const int G = (rows + 31) / 32;
+    return std::max(1, std::min(n, resident / G));
+}
+
 void launch_commit(uint64_t *out, uint4 *part, const uint64_t *poly, const uint4 *table, int rows, int n, int W,
                    int cb, cudaStream_t st) {
-    const unsigned warps = (unsigned)((rows + 31) / 32) * (unsigned)(n / COMMIT_CHUNK);
-    k_commit_partial<<<blocks_for(warps, 4), 128, 0, st>>>(part, poly, table, rows, n, W, cb);
-    k_commit_reduce<<<blocks_for((size_t)rows, 128), 128, 0, st>>>(out, part, rows, n / COMMIT_CHUNK);
+    const int P = commit_parts(rows, n);
+    const unsigned warps = (unsigned)((rows + 31) / 32) * (unsigned)P;
+    k_commit_partial<<<blocks_for(warps, 4), 128, 0, st>>>(part, poly, table, rows, n, W, cb, P);
+    k_commit_reduce<<<blocks_for((size_t)rows, 128), 128, 0, st>>>(out, part, rows, P);
 }
 
 void launch_msm(const MsmArgs &a, int threads, cudaStream_t st) {

@@ -65,8 +65,10 @@ void launch_ref_to_scalars(uint4 *S, const uint64_t *tcf, int rows, int log_m, c
 
 // kernels_msm.cu
 void launch_msm(const MsmArgs &a, int threads, cudaStream_t st);  // threads: 64, 128 or 256
-// KZG commitments: bases per pass-1 warp; part holds (rows/32) x (n/COMMIT_CHUNK) point tiles
+// KZG commitments: polynomial lengths are multiples of COMMIT_CHUNK; pass 1
+// has commit_parts(rows, n) warps per 32 rows, and part holds as many tiles
 constexpr int COMMIT_CHUNK = 32;
+int commit_parts(int rows, int n);
 void launch_commit(uint64_t *out, uint4 *part, const uint64_t *poly, const uint4 *table, int rows, int n, int W,
                    int cb, cudaStream_t st);
 
