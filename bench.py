@@ -536,6 +536,7 @@ def run_serve(args, ws, rank, dev):
         start = time.perf_counter()
         due = start
         warm = args.serve_warmup > 0
+        lag = 0.0  # how far the client fell behind the arrival schedule
         for j in range(count):
             if warm and due - start >= args.serve_warmup:
                 srv.reset_stats()  # steady state: later completions only
@@ -546,8 +547,10 @@ def run_serve(args, ws, rank, dev):
                 time.sleep(d)
             nj = int(lens[j])
             out = free[nj].pop() if free[nj] else np.zeros((nj // 8, 18), np.uint64)
+            lag = max(lag, time.perf_counter() - due)
             t = srv.submit(pool[nj][j % 24], out)
             pending.put((t, nj, j, out))
+        submit_s = time.perf_counter() - start
         pending.put(None)
         th.join()
         st = srv.stats()
@@ -557,7 +560,10 @@ def run_serve(args, ws, rank, dev):
                       "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
                       "max_ms": st["max_ms"], "p99_below_plain_batch_latency": st["p99_ms"] < plain_ms,
                       "mean_pack_rows": st["mean_pack_rows"], "packs": st["packs"],
-                      "errors": sum(1 for r in done_rc if r != 0)})
+                      "errors": sum(1 for r in done_rc if r != 0),
+                      # the load generator itself: requests/s it achieved against the schedule's
+                      "arrivals_per_s": {"offered": rate, "achieved": count / submit_s},
+                      "client_max_lag_ms": lag * 1e3})
     srv.close()
     # served results are the ones the same polynomial gives alone
     same = True
