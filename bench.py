@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--serve-fft-blocks", type=int, default=0,
                     help="persistent-FFT blocks per SM of each pack (0: adaptive to the backlog)")
+    ap.add_argument("--serve-burst-rows", type=int, default=0,
+                    help="pack size while more than 2 x max rows requests wait (0: 7/5 of max rows)")
     ap.add_argument("--serve-latency-rows", type=int, default=0,
                     help="latency-mode packs while at most this many requests wait (0: max rows)")
     ap.add_argument("--autotune", action="store_true", help="autotune the context before timing (batch, ragged)")
@@ -505,7 +507,7 @@ def run_serve(args, ws, rank, dev):
     weights = np.array([w for _, w in SERVE_MIX])
     mean_proofs = float((sizes // 8 * weights).sum())
     srv = E.Server(ctx, max_rows=args.serve_max_rows, slots=args.serve_slots, fft_blocks_per_sm=args.serve_fft_blocks,
-                   latency_rows=args.serve_latency_rows)
+                   latency_rows=args.serve_latency_rows, burst_rows=args.serve_burst_rows)
     loads = []
     rng = np.random.default_rng(42)
     check = []  # (n, pool index, output) kept for the bit-exactness check
@@ -581,7 +583,8 @@ def run_serve(args, ws, rank, dev):
                                "(weights 0.2/0.3/0.5) at fractions of plain-batch capacity",
                    "window_bits": args.window, "max_rows_per_pack": args.serve_max_rows,
                    "slots": args.serve_slots, "fft_blocks_per_sm": args.serve_fft_blocks or "adaptive",
-                   "latency_rows": args.serve_latency_rows or args.serve_max_rows, "arrival_window_s": args.serve_seconds,
+                   "latency_rows": args.serve_latency_rows or args.serve_max_rows,
+                   "burst_rows": args.serve_burst_rows or min(4096, args.serve_max_rows * 7 // 5), "arrival_window_s": args.serve_seconds,
                    "warmup_s_excluded": args.serve_warmup, "setup_s": round(setup_s, 2),
                    "table_bytes": ctx.device_bytes()},
         "plain_batch": {"rows": rows, "n": n, "proofs_per_s": plain_pps, "latency_ms": plain_ms},

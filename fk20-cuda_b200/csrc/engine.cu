@@ -1762,10 +1762,11 @@ void server_main(fk20_server *s) {
             // length; a partial group idles lanes): its youngest extra
             // requests go back to the head of the queue for the next pack.
             const bool latency = s->queue.size() <= s->cfg.latency_rows;
-            const bool more = s->queue.size() > s->cfg.max_rows;
+            const size_t cap = s->queue.size() > 2 * (size_t)s->cfg.max_rows ? s->cfg.burst_rows : s->cfg.max_rows;
+            const bool more = s->queue.size() > cap;
             unsigned cnt[3] = {0, 0, 0};
             size_t q = 0;
-            for (; q < s->queue.size() && fs->reqs.size() < s->cfg.max_rows; q++) {
+            for (; q < s->queue.size() && fs->reqs.size() < cap; q++) {
                 const Req &r = s->queue[q];
                 const int k = log_m_for_n(r.n) - 7;
                 unsigned c2[3] = {cnt[0], cnt[1], cnt[2]};
@@ -1855,6 +1856,8 @@ int fk20_server_create(fk20_server **out, fk20_ctx *ctx, const fk20_server_confi
     if (!c.slots) c.slots = 2;
     if (!c.max_queue) c.max_queue = 1u << 16;
     if (c.max_rows > 4096 || c.slots > 8) return FK20_EINVAL;
+    if (!c.burst_rows) c.burst_rows = std::min(4096u, c.max_rows + c.max_rows * 2 / 5);
+    if (c.burst_rows < c.max_rows || c.burst_rows > 4096) return FK20_EINVAL;
     fk20_server *s = new fk20_server();
     s->ctx = ctx;
     {
@@ -1870,27 +1873,28 @@ int fk20_server_create(fk20_server **out, fk20_ctx *ctx, const fk20_server_confi
         }
         s->slots.resize(c.slots);
         int rc = 0;
-        // Size every slot for a full pack now (max_rows requests of the longest
-        // length, plus a partial group per length) when that fits the budget:
-        // growing a buffer later would synchronise the device and stall the
-        // other slots' packs.
-        const unsigned full[3] = {32, 32, c.max_rows + 32};
+        // Size every slot for a full pack now (burst_rows requests of the
+        // longest length, plus a partial group per length) when that fits the
+        // budget: growing a buffer later would synchronise the device and
+        // stall the other slots' packs.
+        const unsigned cap = c.burst_rows;
+        const unsigned full[3] = {32, 32, cap + 32};
         const bool presize = pack_bytes(full) * c.slots <= c.hbm_budget;
         for (Slot &sl : s->slots) {
             if (!rc && cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) != cudaSuccess) rc = (int)cudaGetLastError();
             if (!rc && cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) rc = (int)cudaGetLastError();
             if (!rc) rc = sl.ws.init();
             if (!rc && presize) {
-                const size_t in_b = (size_t)(c.max_rows + 64) * 4096 * sizeof(fr_t);
-                const size_t out_b = (size_t)(c.max_rows + 64) * 512 * sizeof(g1p_t);
+                const size_t in_b = (size_t)(cap + 64) * 4096 * sizeof(fr_t);
+                const size_t out_b = (size_t)(cap + 64) * 512 * sizeof(g1p_t);
                 const Seg sg[3] = {{7, 32, nullptr, nullptr}, {8, 32, nullptr, nullptr},
-                                   {9, c.max_rows + 32, nullptr, nullptr}};
+                                   {9, cap + 32, nullptr, nullptr}};
                 rc = sl.dpoly.reserve(in_b);
                 if (!rc) rc = sl.dout.reserve(out_b);
                 if (!rc) rc = pinned_reserve(&sl.hpoly, &sl.hpoly_bytes, in_b);
                 if (!rc) rc = pinned_reserve(&sl.hout, &sl.hout_bytes, out_b);
-                if (!rc) rc = sl.ws.stage_offsets(2 * (size_t)(c.max_rows + 64));
-                if (!rc) rc = sl.ws.offs.reserve(2 * (size_t)(c.max_rows + 64) * sizeof(size_t));
+                if (!rc) rc = sl.ws.stage_offsets(2 * (size_t)(cap + 64));
+                if (!rc) rc = sl.ws.offs.reserve(2 * (size_t)(cap + 64) * sizeof(size_t));
                 if (!rc) {
                     SegLayout lay;
                     for (int k = 0; k < 3 && !rc; k++) {

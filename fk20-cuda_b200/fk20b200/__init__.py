@@ -65,7 +65,7 @@ class TuneResult(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("max_rows", ctypes.c_uint), ("slots", ctypes.c_uint), ("hbm_budget", ctypes.c_size_t),
                 ("max_queue", ctypes.c_uint), ("fft_blocks_per_sm", ctypes.c_uint),
-                ("latency_rows", ctypes.c_uint)]
+                ("latency_rows", ctypes.c_uint), ("burst_rows", ctypes.c_uint)]
 
 
 class ServerStats(ctypes.Structure):
@@ -353,8 +353,8 @@ class Server:
     output (n/8 x 18 uint64); both are kept referenced until wait()."""
 
     def __init__(self, ctx: Context, max_rows: int = 0, slots: int = 0, hbm_budget: int = 0, max_queue: int = 0,
-                 fft_blocks_per_sm: int = 0, latency_rows: int = 0):
-        cfg = ServerConfig(max_rows, slots, hbm_budget, max_queue, fft_blocks_per_sm, latency_rows)
+                 fft_blocks_per_sm: int = 0, latency_rows: int = 0, burst_rows: int = 0):
+        cfg = ServerConfig(max_rows, slots, hbm_budget, max_queue, fft_blocks_per_sm, latency_rows, burst_rows)
         h = ctypes.c_void_p()
         call("fk20_server_create", ctypes.byref(h), ctx.h, ctypes.byref(cfg))
         self.h = h

@@ -281,6 +281,8 @@ typedef struct {
     unsigned latency_rows;      /* latency mode while at most this many requests wait: a pack takes them all;
                                    beyond it, throughput mode: packs of up to max_rows, whole 32-row groups per
                                    length (0 = max_rows; <= max_rows) */
+    unsigned burst_rows;        /* pack size while more than 2 max_rows requests wait: larger packs drain a
+                                   backlog faster (0 = 7/5 max_rows, i.e. 224 for 160; max_rows..4096) */
 } fk20_server_config;
 typedef struct {
     uint64_t requests, proofs, packs;
