@@ -5,7 +5,8 @@
 // ate pairing of BLS12 curves computed with the standard techniques:
 //   * Fp2 = Fp[u]/(u^2 + 1), Fp6 = Fp2[v]/(v^3 - xi), Fp12 = Fp6[w]/(w^2 - v),
 //     xi = 1 + u (so w^6 = xi); Karatsuba products at every level (an Fp12
-//     product is 18 Fp2 products, a square 12).
+//     product is 18 Fp2 products, a square 12; a square in the cyclotomic
+//     subgroup, where the final exponentiation works, 9 Fp2 squares).
 //   * G2 on the M-type twist E': y^2 = x^3 + 4 xi, mapped into E(Fp12) by
 //     psi(x', y') = (x'/w^2, y'/w^3).
 //   * Miller loop over the bits of |z| = 0xd201000000010000 with T in
@@ -279,6 +280,50 @@ static __device__ __noinline__ void f12_frob(Fp12 *r, const Fp12 *a, bool conj) 
     }
 }
 
+// x^2 in Fp4 = Fp2[s]/(s^2 - xi) for x = (x0, x1) = x0 + x1 s: (x0^2 + xi x1^2, 2 x0 x1)
+FK_D void f4_sqr(Fp2 &r0, Fp2 &r1, const Fp2 &x0, const Fp2 &x1) {
+    Fp2 a = f2s(x0), b = f2s(x1), t;
+    f2_add(t, x0, x1);
+    t = f2s(t);
+    f2_sub(t, t, a);
+    f2_sub(r1, t, b);
+    f2_xi(b, b);
+    f2_add(r0, a, b);
+}
+// 3 a - 2 b = a + 2 (a - b) and 3 a + 2 b = a + 2 (a + b)
+FK_D void f2_3a_2b(Fp2 &r, const Fp2 &a, const Fp2 &b, bool minus) {
+    Fp2 t;
+    if (minus) f2_sub(t, a, b);
+    else f2_add(t, a, b);
+    f2_add(t, t, t);
+    f2_add(r, a, t);
+}
+// r = a^2 for a in the cyclotomic subgroup (a^(p^6 + 1) = 1, a^(p^4 - p^2 + 1)
+// = 1), as Granger and Scott square there: with Fp12 = Fp4[w]/(w^3 - s),
+// s = w^3, a = g0 + g1 w + g2 w^2 (g0 = (w0, w3), g1 = (w1, w4), g2 = (w2, w5)):
+// a^2 = (3 g0^2 - 2 conj g0) + (3 s g2^2 + 2 conj g1) w + (3 g1^2 - 2 conj g2) w^2,
+// conj the Fp4 conjugate (x0, x1) -> (x0, -x1): 9 Fp2 squares instead of 12
+// Fp2 products; r may alias a
+static __device__ __noinline__ void f12_cyc_sqr(Fp12 *r, const Fp12 *a) {
+    Fp2 A0, A1, B0, B1, C0, C1, o[6];
+    f4_sqr(A0, A1, a->a0.c[0], a->a1.c[1]);
+    f4_sqr(B0, B1, a->a1.c[0], a->a0.c[2]);
+    f4_sqr(C0, C1, a->a0.c[1], a->a1.c[2]);
+    f2_3a_2b(o[0], A0, a->a0.c[0], true);   // w^0
+    f2_3a_2b(o[3], A1, a->a1.c[1], false);  // w^3
+    f2_xi(C1, C1);
+    f2_3a_2b(o[1], C1, a->a1.c[0], false);  // w^1: 3 xi C1 + 2 g1.0
+    f2_3a_2b(o[4], C0, a->a0.c[2], true);   // w^4: 3 C0 - 2 g1.1
+    f2_3a_2b(o[2], B0, a->a0.c[1], true);   // w^2
+    f2_3a_2b(o[5], B1, a->a1.c[2], false);  // w^5
+    r->a0.c[0] = o[0];
+    r->a1.c[0] = o[1];
+    r->a0.c[1] = o[2];
+    r->a1.c[1] = o[3];
+    r->a0.c[2] = o[4];
+    r->a1.c[2] = o[5];
+}
+
 // ---------------------------------------------------------------- Miller loop
 struct G2H {  // homogeneous projective point of the twist
     Fp2 x, y, z;
@@ -387,7 +432,7 @@ static __device__ __noinline__ void exp_z(Fp12 *r, const Fp12 *a) {
     Fp12 acc = *a;
 #pragma unroll 1
     for (int i = 62; i >= 0; i--) {
-        f12_sqr(&acc, &acc);
+        f12_cyc_sqr(&acc, &acc);
         if ((Z_ABS >> i) & 1ull) f12_mul(&acc, &acc, a);
     }
     f12_conj(*r, acc);
@@ -415,7 +460,7 @@ static __device__ __noinline__ void final_exp(Fp12 *r, const Fp12 *f) {
     f12_mul(&c, &c, &t);
     f12_conj(t, b);
     f12_mul(&c, &c, &t);
-    f12_sqr(&t, &m);  // times m^3
+    f12_cyc_sqr(&t, &m);  // times m^3
     f12_mul(&t, &t, &m);
     f12_mul(r, &c, &t);
 }
