@@ -5,8 +5,9 @@
 // ate pairing of BLS12 curves computed with the standard techniques:
 //   * Fp2 = Fp[u]/(u^2 + 1), Fp6 = Fp2[v]/(v^3 - xi), Fp12 = Fp6[w]/(w^2 - v),
 //     xi = 1 + u (so w^6 = xi); Karatsuba products at every level (an Fp12
-//     product is 18 Fp2 products, a square 12; a square in the cyclotomic
-//     subgroup, where the final exponentiation works, 9 Fp2 squares).
+//     product is 18 Fp2 products, a square 12, a product by a line 13; a
+//     square in the cyclotomic subgroup, where the final exponentiation
+//     works, 9 Fp2 squares).
 //   * G2 on the M-type twist E': y^2 = x^3 + 4 xi, mapped into E(Fp12) by
 //     psi(x', y') = (x'/w^2, y'/w^3).
 //   * Miller loop over the bits of |z| = 0xd201000000010000 with T in
@@ -324,20 +325,66 @@ static __device__ __noinline__ void f12_cyc_sqr(Fp12 *r, const Fp12 *a) {
     r->a1.c[2] = o[5];
 }
 
+// r = x (c0 + c1 v): 5 Fp2 products; r may alias x
+FK_D void f6_mul01(Fp6 &r, const Fp6 &x, const Fp2 &c0, const Fp2 &c1) {
+    Fp2 t0 = f2m(x.c[0], c0), t1 = f2m(x.c[1], c1), u, v, r0, r1;
+    u = f2m(x.c[2], c1);
+    f2_xi(u, u);
+    f2_add(r0, t0, u);
+    f2_add(u, x.c[0], x.c[1]);
+    f2_add(v, c0, c1);
+    u = f2m(u, v);
+    f2_sub(u, u, t0);
+    f2_sub(r1, u, t1);
+    u = f2m(x.c[2], c0);
+    f2_add(r.c[2], t1, u);
+    r.c[0] = r0;
+    r.c[1] = r1;
+}
+// r = x (c1 v): 3 Fp2 products; r may alias x
+FK_D void f6_mul1(Fp6 &r, const Fp6 &x, const Fp2 &c1) {
+    Fp2 t = f2m(x.c[2], c1);
+    f2_xi(t, t);
+    r.c[2] = f2m(x.c[1], c1);
+    r.c[1] = f2m(x.c[0], c1);
+    r.c[0] = t;
+}
+// Fp6 sums written out, not as a loop: with the rolled loops of f6_add /
+// f6_sub after the products below, the GPU build of f12_mul_line gave wrong
+// odd coefficients (the same source is right on the host, and right with
+// the sums unrolled or placed before the products)
+FK_D void f6_add3(Fp6 &r, const Fp6 &a, const Fp6 &b) {
+    f2_add(r.c[0], a.c[0], b.c[0]);
+    f2_add(r.c[1], a.c[1], b.c[1]);
+    f2_add(r.c[2], a.c[2], b.c[2]);
+}
+FK_D void f6_sub3(Fp6 &r, const Fp6 &a, const Fp6 &b) {
+    f2_sub(r.c[0], a.c[0], b.c[0]);
+    f2_sub(r.c[1], a.c[1], b.c[1]);
+    f2_sub(r.c[2], a.c[2], b.c[2]);
+}
+// f = f (c0 + c2 w^2 + c3 w^3), l = (c0, c2, c3): the sparse product by a
+// line, 13 Fp2 products instead of 18
+static __device__ __noinline__ void f12_mul_line(Fp12 *f, const Fp2 *l) {
+    Fp6 t0, t1, s;
+    Fp2 c23;
+    f6_mul01(t0, f->a0, l[0], l[1]);
+    f6_mul1(t1, f->a1, l[2]);
+    f6_add3(s, f->a0, f->a1);
+    f2_add(c23, l[1], l[2]);
+    f6_mul01(s, s, l[0], c23);
+    f6_sub3(s, s, t0);
+    f6_sub3(f->a1, s, t1);
+    f6_mulv(t1, t1);
+    f6_add3(f->a0, t0, t1);
+}
+
 // ---------------------------------------------------------------- Miller loop
 struct G2H {  // homogeneous projective point of the twist
     Fp2 x, y, z;
 };
-// the line c0 + c2 w^2 + c3 w^3 as an Fp12 element
-FK_D void line_f12(Fp12 &l, const Fp2 &c0, const Fp2 &c2, const Fp2 &c3) {
-    f6_zero(l.a0);
-    f6_zero(l.a1);
-    l.a0.c[0] = c0;
-    l.a0.c[1] = c2;
-    l.a1.c[1] = c3;
-}
-// T = 2T; l = tangent at T evaluated at P
-static __device__ __noinline__ void dbl_step(G2H *T, Fp12 *l, const Fp *xp, const Fp *yp) {
+// T = 2T; l = (c0, c2, c3) of the tangent at T evaluated at P
+static __device__ __noinline__ void dbl_step(G2H *T, Fp2 *l, const Fp *xp, const Fp *yp) {
     Fp2 B = f2s(T->y), C = f2s(T->z), E, F, XX = f2s(T->x), H, t, u, c2, c3;
     f2_xi(t, C);
     f2_mul12(E, t);  // 3 b' Z^2 = 12 xi Z^2
@@ -351,7 +398,9 @@ static __device__ __noinline__ void dbl_step(G2H *T, Fp12 *l, const Fp *xp, cons
     f2_mul_fp(c2, u, *xp);
     f2_neg(c2, c2);
     f2_mul_fp(c3, H, *yp);
-    line_f12(*l, t, c2, c3);
+    l[0] = t;
+    l[1] = c2;
+    l[2] = c3;
     t = f2m(T->x, T->y);
     f2_add(t, t, t);
     f2_sub(u, B, F);
@@ -365,8 +414,8 @@ static __device__ __noinline__ void dbl_step(G2H *T, Fp12 *l, const Fp *xp, cons
     f2_add(t, t, t);
     f2_add(T->z, t, t);  // 4 B H
 }
-// T = T + Q (Q affine); l = chord through T and Q evaluated at P
-static __device__ __noinline__ void add_step(G2H *T, Fp12 *l, const Fp2 *xq, const Fp2 *yq, const Fp *xp,
+// T = T + Q (Q affine); l = (c0, c2, c3) of the chord through T and Q evaluated at P
+static __device__ __noinline__ void add_step(G2H *T, Fp2 *l, const Fp2 *xq, const Fp2 *yq, const Fp *xp,
                                              const Fp *yp) {
     Fp2 th, la, t, u, c0, c2, c3, C, D, E, F, G, H;
     t = f2m(*yq, T->z);
@@ -379,7 +428,9 @@ static __device__ __noinline__ void add_step(G2H *T, Fp12 *l, const Fp2 *xq, con
     f2_mul_fp(c2, th, *xp);
     f2_neg(c2, c2);
     f2_mul_fp(c3, la, *yp);
-    line_f12(*l, c0, c2, c3);
+    l[0] = c0;
+    l[1] = c2;
+    l[2] = c3;
     C = f2s(th);
     D = f2s(la);
     E = f2m(la, D);
@@ -399,7 +450,7 @@ static __device__ __noinline__ void add_step(G2H *T, Fp12 *l, const Fp2 *xq, con
 // Q affine on the twist, neither infinity)
 static __device__ __noinline__ void miller(Fp12 *f, int n, const Fp *xp, const Fp *yp, const Fp2 *xq, const Fp2 *yq) {
     G2H T[2];
-    Fp12 l;
+    Fp2 l[3];
 #pragma unroll 1
     for (int j = 0; j < n; j++) {
         T[j].x = xq[j];
@@ -412,14 +463,14 @@ static __device__ __noinline__ void miller(Fp12 *f, int n, const Fp *xp, const F
         f12_sqr(f, f);
 #pragma unroll 1
         for (int j = 0; j < n; j++) {
-            dbl_step(&T[j], &l, &xp[j], &yp[j]);
-            f12_mul(f, f, &l);
+            dbl_step(&T[j], l, &xp[j], &yp[j]);
+            f12_mul_line(f, l);
         }
         if ((Z_ABS >> i) & 1ull) {
 #pragma unroll 1
             for (int j = 0; j < n; j++) {
-                add_step(&T[j], &l, &xq[j], &yq[j], &xp[j], &yp[j]);
-                f12_mul(f, f, &l);
+                add_step(&T[j], l, &xq[j], &yq[j], &xp[j], &yp[j]);
+                f12_mul_line(f, l);
             }
         }
     }
