@@ -72,6 +72,149 @@ struct Elem {
 using Fp = Elem<FpDesc>;
 using Fr = Elem<FrDesc>;
 
+// ---------------------------------------------------------------- carry chains
+// Each chain is one inline-PTX statement in device code (chains.inc, written
+// by gen_chains.py): the carry flag CC.CF never has to survive from one asm
+// statement to the next.  Host builds run the portable stand-ins below, which
+// compute the same words.
+template <class F> FK_D void ptx_add(uint32_t *r, const uint32_t *a, const uint32_t *b);
+template <class F> FK_D uint32_t ptx_sub(uint32_t *r, const uint32_t *a, const uint32_t *b);
+template <class F> FK_D uint32_t ptx_sub_mod(uint32_t *r, const uint32_t *t);
+template <class F> FK_D void ptx_row_even(uint32_t *e, const uint32_t *a, uint32_t b);
+template <class F> FK_D void ptx_row_odd(uint32_t *o, const uint32_t *a, uint32_t b, uint32_t c);
+template <class F> FK_D void ptx_red_even(uint32_t *e, uint32_t m);
+template <class F> FK_D void ptx_red_odd(uint32_t *o, uint32_t m);
+template <class F> FK_D void ptx_final(uint32_t *t, const uint32_t *e, const uint32_t *o);
+#if defined(__CUDA_ARCH__)
+#include "chains.inc"
+#endif
+
+// r = a + b; the carry out of the top word is dropped (callers keep sums < 2^(32N))
+template <class F>
+FK_HD void ch_add(uint32_t *r, const uint32_t *a, const uint32_t *b) {
+#if defined(__CUDA_ARCH__)
+    ptx_add<F>(r, a, b);
+#else
+    uint64_t c = 0;
+    for (int i = 0; i < F::N; i++) { c += (uint64_t)a[i] + b[i]; r[i] = (uint32_t)c; c >>= 32; }
+#endif
+}
+
+// r = a - b; returns all ones when a < b, else 0
+template <class F>
+FK_HD uint32_t ch_sub(uint32_t *r, const uint32_t *a, const uint32_t *b) {
+#if defined(__CUDA_ARCH__)
+    return ptx_sub<F>(r, a, b);
+#else
+    uint64_t br = 0;
+    for (int i = 0; i < F::N; i++) { uint64_t d = (uint64_t)a[i] - b[i] - br; r[i] = (uint32_t)d; br = d >> 63; }
+    return br ? 0xffffffffu : 0u;
+#endif
+}
+
+// r = t - modulus; returns all ones when t < modulus, else 0
+template <class F>
+FK_HD uint32_t ch_sub_mod(uint32_t *r, const uint32_t *t) {
+#if defined(__CUDA_ARCH__)
+    return ptx_sub_mod<F>(r, t);
+#else
+    uint32_t m[F::N];
+    for (int i = 0; i < F::N; i++) m[i] = F::mod(i);
+    return ch_sub<F>(r, t, m);
+#endif
+}
+
+// e[0..N-1] += a[j]*b for even j (lo word at j, hi word at j+1); e[N] = carry out
+template <class F>
+FK_HD void ch_row_even(uint32_t *e, const uint32_t *a, uint32_t b) {
+#if defined(__CUDA_ARCH__)
+    ptx_row_even<F>(e, a, b);
+#else
+    uint64_t c = 0;
+    for (int w = 0; w < F::N; w++) {
+        c += (uint64_t)e[w] + ((w & 1) ? mul_hi(a[w - 1], b) : mul_lo(a[w], b));
+        e[w] = (uint32_t)c;
+        c >>= 32;
+    }
+    e[F::N] = (uint32_t)c;
+#endif
+}
+
+// o[0] += c; o[1..N] += a[j]*b for odd j (lo word at j, hi word at j+1);
+// o[N] is written, not read
+template <class F>
+FK_HD void ch_row_odd(uint32_t *o, const uint32_t *a, uint32_t b, uint32_t c) {
+#if defined(__CUDA_ARCH__)
+    ptx_row_odd<F>(o, a, b, c);
+#else
+    uint64_t s = (uint64_t)o[0] + c;
+    o[0] = (uint32_t)s;
+    s >>= 32;
+    for (int w = 1; w < F::N; w++) {
+        s += (uint64_t)o[w] + ((w & 1) ? mul_lo(a[w], b) : mul_hi(a[w - 1], b));
+        o[w] = (uint32_t)s;
+        s >>= 32;
+    }
+    o[F::N] = (uint32_t)(s + mul_hi(a[F::N - 1], b));
+#endif
+}
+
+// e[0..N-1] += m*mod[j] for even j; e[N] += carry out
+template <class F>
+FK_HD void ch_red_even(uint32_t *e, uint32_t m) {
+#if defined(__CUDA_ARCH__)
+    ptx_red_even<F>(e, m);
+#else
+    uint64_t c = 0;
+    for (int w = 0; w < F::N; w++) {
+        c += (uint64_t)e[w] + ((w & 1) ? mul_hi(m, F::mod(w - 1)) : mul_lo(m, F::mod(w)));
+        e[w] = (uint32_t)c;
+        c >>= 32;
+    }
+    e[F::N] += (uint32_t)c;
+#endif
+}
+
+// o[1..N] += m*mod[j] for odd j (o[0] unchanged)
+template <class F>
+FK_HD void ch_red_odd(uint32_t *o, uint32_t m) {
+#if defined(__CUDA_ARCH__)
+    ptx_red_odd<F>(o, m);
+#else
+    uint64_t c = 0;
+    for (int w = 1; w < F::N; w++) {
+        c += (uint64_t)o[w] + ((w & 1) ? mul_lo(m, F::mod(w)) : mul_hi(m, F::mod(w - 1)));
+        o[w] = (uint32_t)c;
+        c >>= 32;
+    }
+    o[F::N] += (uint32_t)c + mul_hi(m, F::mod(F::N - 1));
+#endif
+}
+
+// t[0..N-1] = (e + o) >> 32 over N+1 words
+template <class F>
+FK_HD void ch_final(uint32_t *t, const uint32_t *e, const uint32_t *o) {
+#if defined(__CUDA_ARCH__)
+    ptx_final<F>(t, e, o);
+#else
+    uint64_t c = ((uint64_t)e[0] + o[0]) >> 32;
+    for (int k = 1; k <= F::N; k++) {
+        c += (uint64_t)e[k] + o[k];
+        t[k - 1] = (uint32_t)c;
+        c >>= 32;
+    }
+#endif
+}
+
+// the carry out of e0 + o0
+FK_HD uint32_t ch_carry0(uint32_t e0, uint32_t o0) {
+#if defined(__CUDA_ARCH__)
+    return ptx_carry0(e0, o0);
+#else
+    return (uint32_t)(((uint64_t)e0 + o0) >> 32);
+#endif
+}
+
 // ---------------------------------------------------------------- helpers
 template <class F>
 FK_HD void f_set_zero(Elem<F> &r) {
@@ -106,10 +249,7 @@ template <class F>
 FK_HD void f_reduce_once(uint32_t r[F::N], const uint32_t t[F::N]) {
     constexpr int N = F::N;
     uint32_t s[N];
-    s[0] = sub_cc(t[0], F::mod(0));
-#pragma unroll
-    for (int i = 1; i < N; i++) s[i] = subc_cc(t[i], F::mod(i));
-    uint32_t borrow = subc(0u, 0u);  // 0xffffffff if t < mod
+    const uint32_t borrow = ch_sub_mod<F>(s, t);  // 0xffffffff if t < mod
 #pragma unroll
     for (int i = 0; i < N; i++) r[i] = (t[i] & borrow) | (s[i] & ~borrow);
 }
@@ -142,49 +282,17 @@ FK_HD void f_mul(Elem<F> &r, const Elem<F> &A, const Elem<F> &B) {
 #pragma unroll
     for (int i = 0; i < N; i++) {
         if (i > 0) {
-            const uint32_t bi = B.w[i];
-            // even products into e[0..N]
-            e[0] = mad_lo_cc(a[0], bi, e[0]);
-            e[1] = madc_hi_cc(a[0], bi, e[1]);
-#pragma unroll
-            for (int j = 2; j < N; j += 2) {
-                e[j] = madc_lo_cc(a[j], bi, e[j]);
-                e[j + 1] = madc_hi_cc(a[j], bi, e[j + 1]);
-            }
-            e[N] = addc(0u, 0u);
-            // carry of the previous word-0 sum, then odd products into o[0..N]
-            o[0] = add_cc(o[0], c);
-#pragma unroll
-            for (int j = 1; j < N - 1; j += 2) {
-                o[j] = madc_lo_cc(a[j], bi, o[j]);
-                o[j + 1] = madc_hi_cc(a[j], bi, o[j + 1]);
-            }
-            o[N - 1] = madc_lo_cc(a[N - 1], bi, o[N - 1]);
-            o[N] = madc_hi(a[N - 1], bi, 0u);
+            // even products into e[0..N]; the previous word-0 carry and the
+            // odd products into o[0..N]
+            ch_row_even<F>(e, a, B.w[i]);
+            ch_row_odd<F>(o, a, B.w[i], c);
         }
         // reduction: add m*p, m chosen so that word 0 vanishes
         const uint32_t m = mul_lo(e[0] + o[0], F::M0);
-        e[0] = mad_lo_cc(m, F::mod(0), e[0]);
-        e[1] = madc_hi_cc(m, F::mod(0), e[1]);
-#pragma unroll
-        for (int j = 2; j < N; j += 2) {
-            e[j] = madc_lo_cc(m, F::mod(j), e[j]);
-            e[j + 1] = madc_hi_cc(m, F::mod(j), e[j + 1]);
-        }
-        e[N] = addc(e[N], 0u);
-        o[1] = mad_lo_cc(m, F::mod(1), o[1]);
-        o[2] = madc_hi_cc(m, F::mod(1), o[2]);
-#pragma unroll
-        for (int j = 3; j < N - 1; j += 2) {
-            o[j] = madc_lo_cc(m, F::mod(j), o[j]);
-            o[j + 1] = madc_hi_cc(m, F::mod(j), o[j + 1]);
-        }
-        o[N - 1] = madc_lo_cc(m, F::mod(N - 1), o[N - 1]);
-        o[N] = madc_hi(m, F::mod(N - 1), o[N]);
-
+        ch_red_even<F>(e, m);
+        ch_red_odd<F>(o, m);
         if (i < N - 1) {
-            (void)add_cc(e[0], o[0]);
-            c = addc(0u, 0u);
+            c = ch_carry0(e[0], o[0]);
 #pragma unroll
             for (int k = 0; k < N; k++) {
                 e[k] = e[k + 1];
@@ -196,10 +304,7 @@ FK_HD void f_mul(Elem<F> &r, const Elem<F> &A, const Elem<F> &B) {
     }
     // final: (e + o) >> 32, then one conditional subtraction
     uint32_t t[N];
-    (void)add_cc(e[0], o[0]);
-#pragma unroll
-    for (int k = 1; k < N; k++) t[k - 1] = addc_cc(e[k], o[k]);
-    t[N - 1] = addc(e[N], o[N]);
+    ch_final<F>(t, e, o);
     f_reduce_once<F>(r.w, t);
 }
 
@@ -208,27 +313,19 @@ FK_HD void f_sqr(Elem<F> &r, const Elem<F> &a) { f_mul<F>(r, a, a); }
 
 template <class F>
 FK_HD void f_add(Elem<F> &r, const Elem<F> &a, const Elem<F> &b) {
-    constexpr int N = F::N;
-    uint32_t t[N];
-    t[0] = add_cc(a.w[0], b.w[0]);
-#pragma unroll
-    for (int i = 1; i < N - 1; i++) t[i] = addc_cc(a.w[i], b.w[i]);
-    t[N - 1] = addc(a.w[N - 1], b.w[N - 1]);
+    uint32_t t[F::N];
+    ch_add<F>(t, a.w, b.w);
     f_reduce_once<F>(r.w, t);
 }
 
 template <class F>
 FK_HD void f_sub(Elem<F> &r, const Elem<F> &a, const Elem<F> &b) {
     constexpr int N = F::N;
-    uint32_t t[N];
-    t[0] = sub_cc(a.w[0], b.w[0]);
+    uint32_t t[N], m[N];
+    const uint32_t borrow = ch_sub<F>(t, a.w, b.w);
 #pragma unroll
-    for (int i = 1; i < N; i++) t[i] = subc_cc(a.w[i], b.w[i]);
-    uint32_t borrow = subc(0u, 0u);
-    r.w[0] = add_cc(t[0], F::mod(0) & borrow);
-#pragma unroll
-    for (int i = 1; i < N - 1; i++) r.w[i] = addc_cc(t[i], F::mod(i) & borrow);
-    r.w[N - 1] = addc(t[N - 1], F::mod(N - 1) & borrow);
+    for (int i = 0; i < N; i++) m[i] = F::mod(i) & borrow;
+    ch_add<F>(r.w, t, m);
 }
 
 template <class F>
@@ -303,10 +400,13 @@ FK_HD void f_pow(Elem<F> &r, const Elem<F> &a, const uint32_t *e, int nw) {
 template <class F>
 FK_HD void f_inv(Elem<F> &r, const Elem<F> &a) {
     uint32_t e[F::N];
-    e[0] = sub_cc(F::mod(0), 2u);
+    uint64_t br = 2;
 #pragma unroll
-    for (int i = 1; i < F::N - 1; i++) e[i] = subc_cc(F::mod(i), 0u);
-    e[F::N - 1] = subc(F::mod(F::N - 1), 0u);
+    for (int i = 0; i < F::N; i++) {
+        const uint64_t d = (uint64_t)F::mod(i) - br;
+        e[i] = (uint32_t)d;
+        br = d >> 63;
+    }
     f_pow<F>(r, a, e, F::N);
 }
 

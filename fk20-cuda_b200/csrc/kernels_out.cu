@@ -29,14 +29,9 @@ FK_D void g1_compress48(uint32_t out[12], const G1P &p) {
     f_from_mont(x, a.x);
     f_from_mont(y, a.y);
     // y > (p - 1) / 2  <=>  2y >= p  (2y < 2^383, no overflow of 12 words + carry)
-    uint32_t t[12];
-    t[0] = add_cc(y.w[0], y.w[0]);
-#pragma unroll
-    for (int k = 1; k < 12; k++) t[k] = addc_cc(y.w[k], y.w[k]);
-    (void)sub_cc(t[0], FpDesc::mod(0));
-#pragma unroll
-    for (int k = 1; k < 12; k++) (void)subc_cc(t[k], FpDesc::mod(k));
-    const uint32_t borrow = subc(0u, 0u);  // all ones when 2y < p
+    uint32_t t[12], s[12];
+    ch_add<FpDesc>(t, y.w, y.w);
+    const uint32_t borrow = ch_sub_mod<FpDesc>(s, t);  // all ones when 2y < p
 #pragma unroll
     for (int k = 0; k < 12; k++) out[k] = be32(x.w[11 - k]);
     out[0] |= 0x80u | (borrow ? 0u : 0x20u);

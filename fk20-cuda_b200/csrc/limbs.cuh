@@ -1,15 +1,12 @@
-// limbs.cuh -- 32-bit carry-chain primitives for multi-limb integer arithmetic.
+// limbs.cuh -- qualifiers and single-word helpers for multi-limb integer
+// arithmetic.
 //
-// On the device every primitive is one PTX integer instruction (add.cc, addc,
-// mad.lo.cc, madc.hi.cc, ...): the carry flag CC.CF threads the chain.  The
-// statements are `asm volatile` so the front end keeps a chain's instructions
-// in program order (the flag is invisible to it); ptxas sees the CC
-// dependencies and may interleave independent chains in SASS.
-//
-// The same functions also compile for the host, where a thread-local flag
-// stands in for CC.CF.  The host build is used for the library's own host-side
-// precomputation (twiddle tables, Montgomery constants) and by the CPU unit
-// tests of the field and curve code; kernels always run the PTX.
+// The carry chains themselves (add.cc / addc / mad.lo.cc / madc.hi.cc ...)
+// are not here: each chain is one inline-PTX statement in chains.inc, called
+// through the ch_* functions of field.cuh, because the carry flag CC.CF is
+// invisible to the compiler and must not cross from one asm statement to
+// another.  Host builds of the field code (the library's host-side
+// precomputation and the CPU unit tests) use portable stand-ins.
 #pragma once
 #include <stdint.h>
 
@@ -23,39 +20,13 @@
 
 namespace fk {
 
+FK_HD uint32_t mul_lo(uint32_t a, uint32_t b) { return a * b; }
+FK_HD uint32_t mul_hi(uint32_t a, uint32_t b) {
 #if defined(__CUDA_ARCH__)
-
-FK_D uint32_t add_cc(uint32_t a, uint32_t b) { uint32_t r; asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
-FK_D uint32_t addc_cc(uint32_t a, uint32_t b) { uint32_t r; asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
-FK_D uint32_t addc(uint32_t a, uint32_t b) { uint32_t r; asm volatile("addc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
-FK_D uint32_t sub_cc(uint32_t a, uint32_t b) { uint32_t r; asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
-FK_D uint32_t subc_cc(uint32_t a, uint32_t b) { uint32_t r; asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
-FK_D uint32_t subc(uint32_t a, uint32_t b) { uint32_t r; asm volatile("subc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
-FK_D uint32_t mad_lo_cc(uint32_t a, uint32_t b, uint32_t c) { uint32_t r; asm volatile("mad.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
-FK_D uint32_t madc_lo_cc(uint32_t a, uint32_t b, uint32_t c) { uint32_t r; asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
-FK_D uint32_t mad_hi_cc(uint32_t a, uint32_t b, uint32_t c) { uint32_t r; asm volatile("mad.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
-FK_D uint32_t madc_hi_cc(uint32_t a, uint32_t b, uint32_t c) { uint32_t r; asm volatile("madc.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
-FK_D uint32_t madc_hi(uint32_t a, uint32_t b, uint32_t c) { uint32_t r; asm volatile("madc.hi.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
-FK_D uint32_t mul_lo(uint32_t a, uint32_t b) { return a * b; }
-FK_D uint32_t mul_hi(uint32_t a, uint32_t b) { return __umulhi(a, b); }
-
-#else  // host stand-in for CC.CF
-
-inline uint32_t &host_cf() { static thread_local uint32_t cf = 0; return cf; }
-inline uint32_t add_cc(uint32_t a, uint32_t b) { uint64_t s = (uint64_t)a + b; host_cf() = (uint32_t)(s >> 32); return (uint32_t)s; }
-inline uint32_t addc_cc(uint32_t a, uint32_t b) { uint64_t s = (uint64_t)a + b + host_cf(); host_cf() = (uint32_t)(s >> 32); return (uint32_t)s; }
-inline uint32_t addc(uint32_t a, uint32_t b) { return (uint32_t)((uint64_t)a + b + host_cf()); }
-inline uint32_t sub_cc(uint32_t a, uint32_t b) { uint64_t d = (uint64_t)a - b; host_cf() = (uint32_t)(d >> 63); return (uint32_t)d; }
-inline uint32_t subc_cc(uint32_t a, uint32_t b) { uint64_t d = (uint64_t)a - b - host_cf(); host_cf() = (uint32_t)(d >> 63); return (uint32_t)d; }
-inline uint32_t subc(uint32_t a, uint32_t b) { return (uint32_t)((uint64_t)a - b - host_cf()); }
-inline uint32_t mad_lo_cc(uint32_t a, uint32_t b, uint32_t c) { uint64_t s = (uint64_t)(uint32_t)(a * b) + c; host_cf() = (uint32_t)(s >> 32); return (uint32_t)s; }
-inline uint32_t madc_lo_cc(uint32_t a, uint32_t b, uint32_t c) { uint64_t s = (uint64_t)(uint32_t)(a * b) + c + host_cf(); host_cf() = (uint32_t)(s >> 32); return (uint32_t)s; }
-inline uint32_t mad_hi_cc(uint32_t a, uint32_t b, uint32_t c) { uint64_t s = (((uint64_t)a * b) >> 32) + c; host_cf() = (uint32_t)(s >> 32); return (uint32_t)s; }
-inline uint32_t madc_hi_cc(uint32_t a, uint32_t b, uint32_t c) { uint64_t s = (((uint64_t)a * b) >> 32) + c + host_cf(); host_cf() = (uint32_t)(s >> 32); return (uint32_t)s; }
-inline uint32_t madc_hi(uint32_t a, uint32_t b, uint32_t c) { return (uint32_t)((((uint64_t)a * b) >> 32) + c + host_cf()); }
-inline uint32_t mul_lo(uint32_t a, uint32_t b) { return a * b; }
-inline uint32_t mul_hi(uint32_t a, uint32_t b) { return (uint32_t)(((uint64_t)a * b) >> 32); }
-
+    return __umulhi(a, b);
+#else
+    return (uint32_t)(((uint64_t)a * b) >> 32);
 #endif
+}
 
 }  // namespace fk
