@@ -883,6 +883,7 @@ def run_reference(args, ws, rank):
         step.append(time.time() - t)
     tot = sum(step)
     value = srows * m * args.steps / tot
+    ref_gpu = reference_gpu_leg(args, xext, cores)
     return {
         "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot * 1e3 / args.steps, "higher_is_better": True,
@@ -893,7 +894,59 @@ def run_reference(args, ws, rank):
                          "sample": f"{srows} rows x {n} coefficients per step ({srows * m} proofs) on {cores} "
                                    "threads; FK20Py multi restated in C (py_ecc absent)"},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": ref_gpu,
     }
+
+
+def reference_gpu_leg(args, xext, cores):
+    """The reference's own CUDA pipeline on this GPU, beside its CPU path: the
+    unmodified reference library (oracle/_ref/libfk20ref.so, built from its
+    sources for sm_100a by oracle/ref/Makefile) runs fk20_poly2h_fft
+    (fk20_poly2h_fft.cu:47-78; rows <= 512, l = 16, n = 4096) on the same
+    seeded batch as this benchmark's own arm, timed with CUDA events around the
+    call the way fk20benchmark.cu:103-116 times it.  Two rows of its output are
+    checked against the oracle."""
+    import numpy as np
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libfk20ref.so")
+    if not os.path.exists(lib_path):
+        return {"unavailable": "reference library not built (oracle/ref/Makefile)"}
+    if args.n != 4096 or args.rows > 512:
+        return {"unavailable": "the reference pipeline is fixed at n = 4096 and at most 512 rows"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+    except ImportError:
+        return {"unavailable": "torch not importable"}
+    import ctypes
+    import oracle as O
+    lib = ctypes.CDLL(lib_path, mode=os.RTLD_LOCAL)
+    rows, n, m = args.rows, args.n, 2 * args.n // L
+    poly = seeded_polys(1000, rows, n)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+    dpoly, dxext = dev(poly), dev(xext)
+    out = torch.zeros((rows, m, 18), dtype=torch.int64, device="cuda")
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    ms = ctypes.c_float(0)
+    rc = lib.ref_fk20_time(P(out), P(dpoly), P(dxext), ctypes.c_uint(rows), ctypes.byref(ms))  # warm-up
+    steps = max(1, min(args.steps, 3))
+    times = []
+    for _ in range(steps):
+        if rc:
+            break
+        rc = lib.ref_fk20_time(P(out), P(dpoly), P(dxext), ctypes.c_uint(rows), ctypes.byref(ms))
+        times.append(ms.value)
+    if rc:
+        return {"unavailable": f"reference pipeline returned CUDA error {rc}"}
+    h = out.cpu().numpy().view(np.uint64)
+    check = [0, rows - 1]
+    exp = O.fk20_rows(poly[check], xext, L, cores)
+    same = all(np.array_equal(O.g1_normalize(h[r]), e) for r, e in zip(check, exp))
+    tot = sum(times)
+    return {"ms_per_step": tot / steps, "proofs_per_s": rows * m * steps / (tot * 1e-3), "steps": steps,
+            "rows": rows, "n": n, "rows_checked_against_oracle": check, "same_as_oracle": same,
+            "path": "reference fk20_poly2h_fft (fk20_poly2h_fft.cu:47-78), reference kernels compiled for sm_100a; "
+                    "double-and-add fk20_msm, g1p_ift/g1p_fft wrappers"}
 
 
 def main():
