@@ -67,6 +67,12 @@ def parse():
                     help="pack size while more than 2 x max rows requests wait (0: 7/5 of max rows)")
     ap.add_argument("--serve-latency-rows", type=int, default=0,
                     help="latency-mode packs while at most this many requests wait (0: max rows)")
+    ap.add_argument("--no-records", action="store_true",
+                    help="batch mode at N = 1: skip the served-load and ragged-batch records of the line")
+    ap.add_argument("--record-serve-seconds", type=float, default=6.0,
+                    help="arrival window per load level of the served record (batch mode)")
+    ap.add_argument("--record-serve-loads", default="0.5,0.8,0.9,1.2",
+                    help="load levels of the served record, as fractions of plain-batch capacity (batch mode)")
     ap.add_argument("--autotune", action="store_true", help="autotune the context before timing (batch, ragged)")
     ap.add_argument("--msm-threads", type=int, default=0, help="MSM block size (64, 128, 256; 0 = the context's)")
     ap.add_argument("--tune-max-table-bytes", type=int, default=0,
@@ -439,6 +445,22 @@ def run_ours(args, ws, rank, dev):
                          "C restatement of FK20Py multi (variable-base double-and-add MSM, G1 FFT by scalar "
                          "multiplication), not py_ecc"}
 
+    # ---- the rest of the metric at N = 1: the ragged batch and the served load
+    ragged = served = None
+    if ws == 1 and not args.no_records:
+        del poly, h_fft
+        for n2 in (1024, 2048):
+            if n2 != n:
+                ctx.load_setup(n2, gpu_setup(E, n2))
+        torch.cuda.synchronize()
+        with ClockSampler(dev) as rclk:
+            ragged = ragged_on(ctx, rank, 5, 3)
+        ragged["clocks"] = rclk.summary()
+        with ClockSampler(dev) as sclk:
+            served = serve_on(args, ctx, rank, [float(x) for x in args.record_serve_loads.split(",")],
+                              args.record_serve_seconds, 1.0, total_ms / args.steps)
+        served["clocks"] = sclk.summary()
+
     line = {
         "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -446,7 +468,7 @@ def run_ours(args, ws, rank, dev):
         "config": workload_config(args, {"setup_s": round(setup_s, 2),
                                          "table_bytes": ctx.device_bytes(), "autotune": tune}),
         "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-        "impl": "ours",
+        "ragged": ragged, "served": served, "impl": "ours",
     }
     ctx.close()
     return line
@@ -472,9 +494,6 @@ def run_serve(args, ws, rank, dev):
     capacity, through the continuous-batching server (fk20_server_*); p50/p99
     latency (submit -> proofs in host memory) and sustained proofs/s beside the
     plain 512 x 4096 batch."""
-    import queue
-    import threading
-    import numpy as np
     import torch
     import fk20b200 as E
 
@@ -499,8 +518,36 @@ def run_serve(args, ws, rank, dev):
     e.record()
     e.synchronize()
     plain_ms = s.elapsed_time(e) / 3
-    plain_pps = rows * (2 * n // L) / (plain_ms * 1e-3)
     del poly, h
+    rec = serve_on(args, ctx, rank, [float(x) for x in args.serve_loads.split(",")], args.serve_seconds,
+                   args.serve_warmup, plain_ms)
+    sat = max(rec["loads"], key=lambda x: x["load"])
+    line = {
+        "metric": "served KZG proofs/s, mixed 1024/2048/4096 requests, bit-exact; p50/p99 latency",
+        "value": sat["served_proofs_per_s"], "unit": "proofs/s", "n_gpus": ws, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "mode": "serve",
+        "data": "synthetic (seeded uniform Fr, seeded tau), open-loop Poisson arrivals",
+    }
+    line.update(rec)
+    line["config"]["setup_s"] = round(setup_s, 2)
+    line["impl"] = "ours"
+    ctx.close()
+    return line
+
+
+def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
+    """The served load through a server on `ctx` (setups for 1024, 2048 and
+    4096 loaded): Poisson arrivals at each fraction of the plain batch's
+    capacity (512 x 4096 proofs in plain_ms), `seconds` of arrivals per level
+    after `warmup_s` left out of the statistics; sampled results compared with
+    the same polynomial proved alone."""
+    import queue
+    import threading
+    import numpy as np
+    import fk20b200 as E
+
+    rows, n = args.rows, args.n
+    plain_pps = rows * (2 * n // L) / (plain_ms * 1e-3)
     # request pool: seeded polynomials per length, reused round-robin
     pool = {n: [np.ascontiguousarray(p) for p in seeded_polys(5000 + n, 24, n)] for n, _ in SERVE_MIX}
     sizes = np.array([n for n, _ in SERVE_MIX])
@@ -511,14 +558,15 @@ def run_serve(args, ws, rank, dev):
     loads = []
     rng = np.random.default_rng(42)
     check = []  # (n, pool index, output) kept for the bit-exactness check
-    for frac in [float(x) for x in args.serve_loads.split(",")]:
+    for frac in loads_frac:
         rate = frac * plain_pps / mean_proofs  # requests per second
-        count = max(1, int(rate * (args.serve_seconds + args.serve_warmup)))
+        count = max(1, int(rate * (seconds + warmup_s)))
         gaps = rng.exponential(1.0 / rate, count)
         lens = rng.choice(sizes, count, p=weights)
         free = {int(n): [] for n in sizes}
         pending = queue.Queue()
         done_rc = []
+        level_checks = []
 
         def collector():
             while True:
@@ -527,8 +575,8 @@ def run_serve(args, ws, rank, dev):
                     return
                 t, nj, j, out = item
                 done_rc.append(srv.wait(t, 120000))
-                if len(check) < 24 and j % 5 == 0:
-                    check.append((nj, j % 24, out))
+                if len(level_checks) < 8 and j % 5 == 0:
+                    level_checks.append((nj, j % 24, out))
                 else:
                     free[nj].append(out)
 
@@ -537,10 +585,10 @@ def run_serve(args, ws, rank, dev):
         srv.reset_stats()
         start = time.perf_counter()
         due = start
-        warm = args.serve_warmup > 0
+        warm = warmup_s > 0
         lag = 0.0  # how far the client fell behind the arrival schedule
         for j in range(count):
-            if warm and due - start >= args.serve_warmup:
+            if warm and due - start >= warmup_s:
                 srv.reset_stats()  # steady state: later completions only
                 warm = False
             due += gaps[j]
@@ -556,6 +604,7 @@ def run_serve(args, ws, rank, dev):
         pending.put(None)
         th.join()
         st = srv.stats()
+        check += level_checks
         loads.append({"load": frac, "requests": count, "offered_proofs_per_s": rate * mean_proofs,
                       "served_proofs_per_s": st["proofs_per_s"],
                       "served_vs_plain": st["proofs_per_s"] / plain_pps,
@@ -573,19 +622,14 @@ def run_serve(args, ws, rank, dev):
         hh = E.empty((1, nj // 8, 18))
         ctx.poly2h_fft(hh, E.to_device(pool[nj][j].reshape(1, nj, 4)), 1, nj)
         same &= bool(np.array_equal(E.to_host(hh)[0], out))
-    sat = max(loads, key=lambda x: x["load"])
-    line = {
-        "metric": "served KZG proofs/s, mixed 1024/2048/4096 requests, bit-exact; p50/p99 latency",
-        "value": sat["served_proofs_per_s"], "unit": "proofs/s", "n_gpus": ws, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "mode": "serve",
-        "data": "synthetic (seeded uniform Fr, seeded tau), open-loop Poisson arrivals",
+    return {
         "config": {"workload": "served load: Poisson arrivals of 1024/2048/4096-coefficient requests "
                                "(weights 0.2/0.3/0.5) at fractions of plain-batch capacity",
                    "window_bits": args.window, "max_rows_per_pack": args.serve_max_rows,
                    "slots": args.serve_slots, "fft_blocks_per_sm": args.serve_fft_blocks or "adaptive",
                    "latency_rows": args.serve_latency_rows or args.serve_max_rows,
-                   "burst_rows": args.serve_burst_rows or min(4096, args.serve_max_rows * 7 // 5), "arrival_window_s": args.serve_seconds,
-                   "warmup_s_excluded": args.serve_warmup, "setup_s": round(setup_s, 2),
+                   "burst_rows": args.serve_burst_rows or min(4096, args.serve_max_rows * 7 // 5),
+                   "arrival_window_s": seconds, "warmup_s_excluded": warmup_s,
                    "table_bytes": ctx.device_bytes()},
         "plain_batch": {"rows": rows, "n": n, "proofs_per_s": plain_pps, "latency_ms": plain_ms},
         "loads": loads,
@@ -593,10 +637,7 @@ def run_serve(args, ws, rank, dev):
         "loads_at_80pct_with_p99_below_plain": [x["load"] for x in loads
                                                  if x["served_vs_plain"] >= 0.8 and x["p99_below_plain_batch_latency"]],
         "results_same_alone_and_served": same, "checked_requests": len(check),
-        "impl": "ours",
     }
-    ctx.close()
-    return line
 
 
 # ------------------------------------------------------------------ ragged batch (graph)
@@ -605,7 +646,6 @@ def run_ragged(args, ws, rank, dev):
     setup: one ragged batch (one MSM launch + one persistent G1 FFT launch over
     the three lengths) captured once in a CUDA graph and replayed; checked
     against the plain per-length path."""
-    import numpy as np
     import torch
     import fk20b200 as E
 
@@ -613,6 +653,34 @@ def run_ragged(args, ws, rank, dev):
     ctx = E.Context(dev, args.window)
     for n in (1024, 2048, 4096):
         ctx.load_setup(n, gpu_setup(E, n))
+    tune = None
+    if args.autotune:
+        tune = ctx.autotune(4096, rows=128, max_table_bytes=0)
+    rec = ragged_on(ctx, rank, args.steps, args.warmup, ws)
+    line = {
+        "metric": "KZG proofs/s, ragged batch of 1000 instances (1024/2048/4096), bit-exact",
+        "value": rec.pop("value"), "unit": "proofs/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": rec.pop("ms_per_step"), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "mode": "ragged",
+        "data": "synthetic (seeded uniform Fr, seeded tau)",
+    }
+    line.update(rec)
+    line["config"]["window_bits"] = args.window
+    line["autotune"] = tune
+    line["impl"] = "ours"
+    ctx.close()
+    return line
+
+
+def ragged_on(ctx, rank, steps, warmup, ws=1):
+    """The ragged batch on `ctx` (setups for 1024, 2048 and 4096 loaded): 1000
+    instances as one CUDA-graph plan, `steps` timed replays (L2 flushed between
+    them), then the graph output against a direct call and the per-length
+    plain path."""
+    import numpy as np
+    import torch
+    import fk20b200 as E
+
     rng = np.random.default_rng(77 + rank)
     sizes = [int(x) for x in rng.choice([1024, 2048, 4096], 1000)]
     poly_off, out_off, po, oo = [], [], 0, 0
@@ -623,18 +691,15 @@ def run_ragged(args, ws, rank, dev):
         oo += n // 8
     polys = E.to_device(seeded_fr(31 + rank, po))
     out = E.empty((oo, 18))
-    tune = None
-    if args.autotune:
-        tune = ctx.autotune(4096, rows=128, max_table_bytes=0)
     plan = E.Plan(ctx, out, polys, sizes, poly_off, out_off)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         plan.launch()
     torch.cuda.synchronize()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     barrier(ws)
     ms = []
     stream = torch.cuda.current_stream()
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush.fill_(1)
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
@@ -656,22 +721,16 @@ def run_ragged(args, ws, rank, dev):
         for r, j in enumerate(idx):
             exp[out_off[j]:out_off[j] + n // 8] = h[r]
     torch.cuda.synchronize()
-    proofs = oo
-    line = {
-        "metric": "KZG proofs/s, ragged batch of 1000 instances (1024/2048/4096), bit-exact",
-        "value": ws * proofs * args.steps / (total * 1e-3), "unit": "proofs/s", "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "mode": "ragged",
-        "data": "synthetic (seeded uniform Fr, seeded tau)",
+    rec = {
+        "value": ws * oo * steps / (total * 1e-3), "ms_per_step": total / steps, "steps": steps, "warmup": warmup,
         "config": {"workload": "1000 FK20 instances, lengths uniform over {1024, 2048, 4096}, one CUDA-graph "
-                               "replay per step", "window_bits": args.window, "proofs_per_step": proofs,
+                               "replay per step", "proofs_per_step": oo,
+                   "instances": {str(n): sizes.count(n) for n in (1024, 2048, 4096)},
                    "l2": "flushed between timed steps (256 MiB write)"},
         "graph_equals_direct": bool(torch.equal(out, direct)), "equals_per_length_path": bool(torch.equal(out, exp)),
-        "autotune": tune, "impl": "ours",
     }
     plan.close()
-    ctx.close()
-    return line
+    return rec
 
 
 # ------------------------------------------------------------------ kernel microbenchmarks

@@ -361,10 +361,16 @@ struct DeviceGuard {  // make ctx->device current for the duration of a call
 // MSM's mixed addition into an XYZZ accumulator 10 (8 M + 2 S)
 constexpr double MP = 300.0, MR = 136.0, ADD_P = 12 * MP, MADD_P = 10 * MP, DBL_P = 8 * MP;
 
+// A twiddle program (scalar_prog.cuh): 2P, 3P, 5P, 7P with the complete
+// projective formulas (1 doubling + 3 additions: 44), the four points made
+// affine on the isomorphic curve with their phi images (27) and the result
+// brought back (4), then Jacobian doublings of 7 and mixed additions of 11
+// for the digits (program_cost counts the precompute's doubling and three
+// additions with them).
 double prog_products(int idx) {
     const HostConsts &hc = host_consts();
     if (hc.prog[idx][0] & 0x300u) return 0.0;
-    return hc.prog_dbl[idx] * DBL_P + hc.prog_add[idx] * ADD_P + PROG_SLOTS * MP;  // + beta x of P, 3P, 5P, 7P
+    return (44.0 + 31.0 + 7.0 * (hc.prog_dbl[idx] - 1) + 11.0 * (hc.prog_add[idx] - 3)) * MP;
 }
 
 // one stage over `rows` rows: kind 0 DIF inverse, 1 DIT forward
@@ -1642,7 +1648,7 @@ struct fk20_server {
     std::thread worker;
     // statistics since the last reset
     std::vector<double> lat_ms;
-    uint64_t proofs = 0, packs = 0, pack_rows = 0;
+    uint64_t proofs = 0, packs = 0, pack_rows = 0, rejected = 0, nomem = 0;
     Clock::time_point first, last;
     bool started = false;
 };
@@ -1764,6 +1770,20 @@ void server_main(fk20_server *s) {
             const bool latency = s->queue.size() <= s->cfg.latency_rows;
             const size_t cap = s->queue.size() > 2 * (size_t)s->cfg.max_rows ? s->cfg.burst_rows : s->cfg.max_rows;
             const bool more = s->queue.size() > cap;
+            // Admission by device memory: the packs in flight and this one stay
+            // within the budget, and whatever this pack adds to its slot's
+            // buffers must be free on the device now (less a reserve for the
+            // runtime and other users of the GPU).
+            size_t limit = s->cfg.hbm_budget;
+            {
+                size_t fr = 0, tot = 0;
+                if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+                    const size_t reserve = (size_t)256 << 20;
+                    limit = std::min(limit, others + fs->bytes() + (fr > reserve ? fr - reserve : 0));
+                } else {
+                    cudaGetLastError();
+                }
+            }
             unsigned cnt[3] = {0, 0, 0};
             size_t q = 0;
             for (; q < s->queue.size() && fs->reqs.size() < cap; q++) {
@@ -1771,7 +1791,7 @@ void server_main(fk20_server *s) {
                 const int k = log_m_for_n(r.n) - 7;
                 unsigned c2[3] = {cnt[0], cnt[1], cnt[2]};
                 c2[k]++;
-                if (others + std::max(fs->bytes(), pack_bytes(c2)) > s->cfg.hbm_budget) break;
+                if (others + std::max(fs->bytes(), pack_bytes(c2)) > limit) break;
                 cnt[k]++;
                 fs->reqs.push_back(r);
             }
@@ -1799,6 +1819,7 @@ void server_main(fk20_server *s) {
                 for (Slot &sl : s->slots) busy |= !sl.reqs.empty();
                 if (!busy) {
                     s->finished[s->queue.front().ticket] = FK20_ENOMEM;
+                    s->nomem++;
                     s->queue.pop_front();
                     s->cv_done.notify_all();
                 } else {
@@ -1929,7 +1950,10 @@ int fk20_server_submit(fk20_server *s, const fr_t *poly, unsigned n, g1p_t *h_ff
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stop) return FK20_EINVAL;
-        if (s->queue.size() >= s->cfg.max_queue) return FK20_EAGAIN;
+        if (s->queue.size() >= s->cfg.max_queue) {
+            s->rejected++;
+            return FK20_EAGAIN;
+        }
         const Clock::time_point now = Clock::now();
         const uint64_t t = s->next_ticket++;
         s->queue.push_back(Req{t, poly, n, h_fft, now});
@@ -1974,6 +1998,8 @@ int fk20_server_get_stats(fk20_server *s, fk20_server_stats *out) {
         st.proofs_per_s = st.wall_s > 0 ? s->proofs / st.wall_s : 0;
     }
     st.mean_pack_rows = s->packs ? (double)s->pack_rows / s->packs : 0;
+    st.rejected = s->rejected;
+    st.nomem = s->nomem;
     *out = st;
     return 0;
 }
@@ -1982,7 +2008,7 @@ int fk20_server_reset_stats(fk20_server *s) {
     if (!s) return FK20_EINVAL;
     std::lock_guard<std::mutex> lk(s->mu);
     s->lat_ms.clear();
-    s->proofs = s->packs = s->pack_rows = 0;
+    s->proofs = s->packs = s->pack_rows = s->rejected = s->nomem = 0;
     s->started = false;
     return 0;
 }

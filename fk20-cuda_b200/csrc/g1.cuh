@@ -205,6 +205,80 @@ FK_HD void g1_dbl(G1P &R, const G1P &P) {
     R.z = Z3;
 }
 
+// ---------------------------------------------------------------- Jacobian, a = 0
+// Jacobian coordinates (x = X/Z^2, y = Y/Z^3), used inside the fixed-scalar
+// programs (scalar_prog.cuh).  The formulas below do not involve the curve
+// constant b, so they hold on every curve y^2 = x^3 + b' -- in particular on
+// the isomorphic curve b' = b u^6 on which a program's precomputed points are
+// affine.
+struct G1J {
+    Fp x, y, z;
+};
+
+// R = 2P (2 M + 5 S, "dbl-2009-l" of the Explicit-Formulas Database); R may
+// alias P.  Infinity (Z = 0) stays infinity; no other exceptional input on a
+// curve without points of order 2.
+FK_HD void g1j_dbl(G1J &R, const G1J &P) {
+    Fp A, B, C, D, t;
+    fp_mul(t, P.y, P.z);  // Y Z
+    fp_sqr(B, P.y);       // B = Y^2
+    fp_sqr(A, P.x);       // A = X^2
+    fp_sqr(C, B);         // C = Y^4
+    f_add(D, P.x, B);
+    fp_sqr(D, D);
+    f_sub(D, D, A);
+    f_sub(D, D, C);
+    f_add(D, D, D);       // D = 2 ((X + B)^2 - A - C) = 4 X Y^2
+    f_add(R.z, t, t);     // Z3 = 2 Y Z
+    f_add(t, A, A);
+    f_add(A, t, A);       // E = 3 A
+    fp_sqr(t, A);         // F = E^2
+    f_sub(t, t, D);
+    f_sub(R.x, t, D);     // X3 = F - 2 D
+    f_sub(t, D, R.x);
+    fp_mul(t, A, t);      // E (D - X3)
+    f_add(C, C, C);
+    f_add(C, C, C);
+    f_add(C, C, C);       // 8 C
+    f_sub(R.y, t, C);     // Y3 = E (D - X3) - 8 C
+}
+
+// R = P + (negQ ? -Q : Q) with Q = (x, y) affine, read through an accessor
+// (get(0) = x, get(1) = y); 8 M + 3 S ("madd-2007-bl" with Z3 = 2 Z1 H).
+// NOT complete: P = +-Q (H = 0) and P = infinity give wrong results.  The
+// fixed-scalar programs never meet either for points of order r (a CPU test
+// checks every program's partial sums); R may alias P.
+template <class QT>
+FK_HD void g1j_madd(G1J &R, const G1J &P, const QT &Q, bool negQ) {
+    Fp zz, u, s, h, t, j;
+    fp_sqr(zz, P.z);       // Z1^2
+    Q.get(0, t);
+    fp_mul(u, t, zz);      // U2 = X2 Z1^2
+    fp_mul(s, P.z, zz);    // Z1^3
+    Q.get(1, t);
+    fp_mul(s, t, s);       // S2 = Y2 Z1^3
+    if (negQ) f_neg(s, s);
+    f_sub(h, u, P.x);      // H = U2 - X1
+    fp_mul(t, P.z, h);
+    f_add(R.z, t, t);      // Z3 = 2 Z1 H
+    fp_sqr(t, h);
+    f_add(t, t, t);
+    f_add(t, t, t);        // I = 4 H^2
+    fp_mul(j, h, t);       // J = H I
+    fp_mul(u, P.x, t);     // V = X1 I
+    f_sub(s, s, P.y);
+    f_add(s, s, s);        // r = 2 (S2 - Y1)
+    fp_mul(t, P.y, j);     // Y1 J
+    fp_sqr(h, s);
+    f_sub(h, h, j);
+    f_sub(h, h, u);
+    f_sub(R.x, h, u);      // X3 = r^2 - J - 2 V
+    f_sub(u, u, R.x);
+    fp_mul(u, s, u);       // r (V - X3)
+    f_add(t, t, t);
+    f_sub(R.y, u, t);      // Y3 = r (V - X3) - 2 Y1 J
+}
+
 // affine normalisation in Montgomery form: (x, y, 1) or infinity (0, 1, 0)
 FK_HD void g1_normalize(G1P &p) {
     if (f_is_zero(p.z)) {

@@ -33,38 +33,57 @@ constexpr int PROG_SLOTS = 4;                         // P, 3P, 5P, 7P
 constexpr int PROG_SLOT_WORDS = 36 * PROG_SLOTS + 12 * PROG_SLOTS;  // + beta x of each
 
 // The executor's scratch: for each thread PROG_SLOT_WORDS 32-bit words at
-// base[0], base[stride], ...: point i (x, y, z) at word 36 i, beta x_i at
-// word 144 + 12 i.  Addresses are formed when used, so the scratch costs one
-// pointer of registers.
+// base[0], base[stride], ...  While P, 3P, 5P, 7P are formed, point i is
+// projective (X, Y, Z) at word 36 i.  The main loop then reads point i as
+// (x', y', beta x') at words 36 i, 36 i + 12, 36 i + 24 -- affine coordinates
+// on an isomorphic curve, see g1_mul_prog -- and the scale factor u at word
+// 144.  Addresses are formed when used, so the scratch costs one pointer of
+// registers.
 struct ProgSlots {
     uint32_t *base;
     int stride;
     FK_HD StridedPoint pt(int i) const { return StridedPoint{base + 36 * i * stride, stride}; }
     FK_HD StridedPoint operator[](int i) const { return pt(i); }
-    FK_HD uint32_t *bx(int i) const { return base + (36 * PROG_SLOTS + 12 * i) * stride; }
+    FK_HD uint32_t *word(int w) const { return base + w * stride; }
 };
 
-// Q = point i of the slots or its image phi(Q) = (beta x, y, z): x read from
-// one of two places, y and z shared
-struct SlotQ {
-    const uint32_t *x, *yz;
-    int stride;
-    FK_HD void get(int c, Fp &f) const {
-        const uint32_t *src = c == 0 ? x : yz + 12 * (c - 1) * stride;
+FK_HD void slot_put(uint32_t *dst, int stride, const Fp &f) {
 #pragma unroll
-        for (int k = 0; k < 12; k++) f.w[k] = src[k * stride];
-    }
-    FK_HD void load(G1P &p) const {
-        get(0, p.x);
-        get(1, p.y);
-        get(2, p.z);
-    }
+    for (int k = 0; k < 12; k++) dst[k * stride] = f.w[k];
+}
+FK_HD void slot_get(Fp &f, const uint32_t *src, int stride) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) f.w[k] = src[k * stride];
+}
+
+// Q = point i of the main loop's table or its image phi(Q) = (beta x', y'):
+// x read from one of two places, y shared
+struct SlotQ {
+    const uint32_t *x, *y;
+    int stride;
+    FK_HD void get(int c, Fp &f) const { slot_get(f, c == 0 ? x : y, stride); }
 };
 
-// acc = [k] P for the program of k (P in the prime-order subgroup).  P is
-// read from point 0 of the slots; points 1..3 receive 3P, 5P, 7P and the
-// beta x rows the x of phi(P), phi(3P), phi(5P), phi(7P).  Only the
-// accumulator lives in registers.
+// acc = [k] P for the program of k (P in the prime-order subgroup, or P =
+// infinity), P read from point 0 of the slots, result in homogeneous
+// projective coordinates.
+//
+// 1. 2P, 3P = P + 2P, 5P, 7P with the complete projective formulas.
+// 2. The four points are made affine without an inversion, on the isomorphic
+//    curve E': y^2 = x^3 + b u^6 with u = Z_P Z_3P Z_5P Z_7P, which
+//    (x, y) -> (u^2 x, u^3 y) maps them to: x'_i = X_i u (u / Z_i),
+//    y'_i = Y_i u^2 (u / Z_i) (the products u / Z_i of the other three Z).
+//    phi commutes with the isomorphism, so phi of a table point is
+//    (beta x', y') there too.
+// 3. The digits run on E' with a Jacobian accumulator: doublings of 7 and
+//    mixed additions of 11 Fp products (instead of 8 and 12 for the complete
+//    projective formulas), as neither formula uses b.  The mixed addition is
+//    not complete; for points of order r the accumulator never equals the
+//    added point or its negative, nor infinity (the program's partial sums,
+//    checked on the CPU for every program the library builds).
+// 4. Back to E: Jacobian (X, Y, Z u), i.e. homogeneous (X Z', Y, Z'^3) with
+//    Z' = Z u.  P = infinity (u = 0) makes every value above meaningless;
+//    the lane's flag then selects infinity.
 template <class ProgPtr>
 FK_HD void g1_mul_prog(G1P &acc, const ProgSlots &slot, ProgPtr prog) {
     const uint32_t hdr = prog[0];
@@ -75,9 +94,12 @@ FK_HD void g1_mul_prog(G1P &acc, const ProgSlots &slot, ProgPtr prog) {
         if (negate) f_neg(acc.y, acc.y);
         return;
     }
+    const int st = slot.stride;
+    bool inf;
     {
         // 2P parked in point 3; 3P = P + 2P, 5P = 3P + 2P, 7P = 5P + 2P
         slot.pt(0).load(acc);
+        inf = f_is_zero(acc.z);
         g1_dbl(acc, acc);
         slot.pt(3).put(acc);
         slot.pt(0).load(acc);
@@ -86,40 +108,82 @@ FK_HD void g1_mul_prog(G1P &acc, const ProgSlots &slot, ProgPtr prog) {
             g1_add_q(acc, acc, slot.pt(3), false);
             slot.pt(i).put(acc);
         }
-        Fp beta, x;
+    }
+    {
+        // u = Z0 Z1 Z2 Z3; lambda_i = u / Z_i written over Z_i
+        Fp z0, z1, z2, z3, a, b, t;
+        slot_get(z0, slot.word(24), st);
+        slot_get(z1, slot.word(36 + 24), st);
+        slot_get(z2, slot.word(72 + 24), st);
+        slot_get(z3, slot.word(108 + 24), st);
+        fp_mul(a, z0, z1);
+        fp_mul(b, z2, z3);
+        fp_mul(t, z1, b);
+        slot_put(slot.word(24), st, t);
+        fp_mul(t, z0, b);
+        slot_put(slot.word(36 + 24), st, t);
+        fp_mul(t, a, z3);
+        slot_put(slot.word(72 + 24), st, t);
+        fp_mul(t, a, z2);
+        slot_put(slot.word(108 + 24), st, t);
+        fp_mul(t, a, b);
+        slot_put(slot.word(144), st, t);
+    }
+    {
+        Fp u, beta, m, c;
+        slot_get(u, slot.word(144), st);
 #pragma unroll
         for (int i = 0; i < 12; i++) beta.w[i] = beta_mont(i);
 #pragma unroll 1
         for (int i = 0; i < PROG_SLOTS; i++) {
-            slot.pt(i).get(0, x);
-            fp_mul(x, x, beta);
-            uint32_t *dst = slot.bx(i);
-#pragma unroll
-            for (int k = 0; k < 12; k++) dst[k * slot.stride] = x.w[k];
+            uint32_t *p = slot.word(36 * i);
+            slot_get(m, p + 24 * st, st);
+            fp_mul(m, u, m);  // u lambda_i
+            slot_get(c, p, st);
+            fp_mul(c, c, m);  // x'_i
+            slot_put(p, st, c);
+            fp_mul(c, c, beta);
+            slot_put(p + 24 * st, st, c);  // beta x'_i
+            fp_mul(m, m, u);  // u^2 lambda_i
+            slot_get(c, p + 12 * st, st);
+            fp_mul(c, c, m);  // y'_i
+            slot_put(p + 12 * st, st, c);
         }
     }
+    G1J j;
     const int top = (int)(hdr & 0xffu);
     bool started = false;
     for (int pos = top; pos >= 0; pos--) {
-        if (started) g1_dbl(acc, acc);
+        if (started) g1j_dbl(j, j);
         const uint32_t byte = (prog[1 + (pos >> 2)] >> ((pos & 3) * 8)) & 0xffu;
         for (int h = 0; h < 2; h++) {
             const uint32_t d = (byte >> (4 * h)) & 15u;
             if (d & 1u) {
-                const int i = (int)(d >> 2);
-                const uint32_t *pt = slot.base + 36 * i * slot.stride;
-                const SlotQ q{h ? slot.bx(i) : pt, pt + 12 * slot.stride, slot.stride};
+                const uint32_t *pt = slot.word(36 * (int)(d >> 2));
+                const SlotQ q{h ? pt + 24 * st : pt, pt + 12 * st, st};
                 if (started) {
-                    g1_add_q(acc, acc, q, (d & 2u) != 0);
+                    g1j_madd(j, j, q, (d & 2u) != 0);
                 } else {
-                    q.load(acc);
-                    if (d & 2u) f_neg(acc.y, acc.y);
+                    q.get(0, j.x);
+                    q.get(1, j.y);
+                    if (d & 2u) f_neg(j.y, j.y);
+                    f_set_one(j.z);
                 }
                 started = true;
             }
         }
     }
-    if (negate) f_neg(acc.y, acc.y);
+    if (negate) f_neg(j.y, j.y);
+    {
+        Fp u, t;
+        slot_get(u, slot.word(144), st);
+        fp_mul(j.z, j.z, u);  // Z' = Z u
+        fp_mul(acc.x, j.x, j.z);
+        fp_sqr(t, j.z);
+        fp_mul(acc.z, t, j.z);
+        acc.y = j.y;
+    }
+    if (inf) g1_set_inf(acc);
 }
 
 // register-only convenience form (setup-time and element-wise kernels): a
@@ -247,7 +311,7 @@ inline void make_program(uint32_t prog[PROG_WORDS], const uint64_t k[4]) {
     int d0, a0, d1, a1;
     program_cost(prog, &d0, &a0);
     program_cost(alt, &d1, &a1);
-    if (8 * d1 + 12 * a1 < 8 * d0 + 12 * a0) {
+    if (7 * d1 + 11 * a1 < 7 * d0 + 11 * a0) {
         alt[0] |= 0x400u;
         for (int i = 0; i < PROG_WORDS; i++) prog[i] = alt[i];
     }

@@ -272,7 +272,9 @@ typedef struct fk20_server fk20_server;
 typedef struct {
     unsigned max_rows;  /* requests per pack (1..4096; 0 = 160) */
     unsigned slots;     /* packs in flight at once (1..8; 0 = 2) */
-    size_t hbm_budget;  /* device bytes all slots' buffers may hold (0 = half the free memory at creation) */
+    size_t hbm_budget;  /* device bytes all slots' buffers may hold (0 = half the free memory at creation);
+                           a pack is also admitted only while what it adds to its slot's buffers is free
+                           on the device when it is formed (less a 256 MiB reserve) */
     unsigned max_queue; /* waiting requests beyond which submit returns FK20_EAGAIN (0 = 1 << 16) */
     unsigned fft_blocks_per_sm; /* persistent-FFT blocks per SM of each pack.  0 = adaptive: the kernel's
                                    occupancy in latency mode (a pack may fill the GPU, and the next one's blocks
@@ -290,6 +292,8 @@ typedef struct {
     double wall_s;                          /* first submit -> last completion since the last reset */
     double proofs_per_s;                    /* proofs / wall_s */
     double mean_pack_rows;
+    uint64_t rejected; /* submits refused with FK20_EAGAIN (max_queue requests waiting) */
+    uint64_t nomem;    /* requests failed with FK20_ENOMEM (too large for the device memory alone) */
 } fk20_server_stats;
 int fk20_server_create(fk20_server **srv, fk20_ctx *ctx, const fk20_server_config *cfg);
 /* poly: HOST array of n fr_t (n in 1024, 2048, 4096); h_fft: HOST array of

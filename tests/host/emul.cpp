@@ -96,6 +96,14 @@ int emul_g1_mul_prog(uint64_t *out, const uint64_t *pts, const uint64_t *k, long
 }
 }
 
+extern "C" {
+// the program words host::make_program builds for k (standard form, 4 x u64)
+int emul_make_program(uint32_t *prog, const uint64_t *k) {
+    host::make_program(prog, k);
+    return PROG_WORDS;
+}
+}
+
 #include "fused_plan.cuh"
 extern "C" {
 // The persistent G1 FFT's task schedule for nseg segments (G[k] row groups,

@@ -98,3 +98,53 @@ def test_server_close_finishes_pending_requests(engine, served_ctx):
         h = engine.empty((1, n // 8, 18))
         served_ctx.poly2h_fft(h, engine.to_device(polys[j].reshape(1, n, 4)), 1, n)
         assert np.array_equal(engine.to_host(h)[0], outs[j]), j
+
+
+def test_server_memory_budget_limits_packs(engine, served_ctx):
+    """Admission by device memory: with a budget of 40 MiB for both slots'
+    buffers (a 4096-coefficient request needs ~10 MiB of tiles for its 32-row
+    group), the 40 requests submitted at once cannot form one pack; they are
+    proved in several, every one of them exact."""
+    rng = np.random.default_rng(8)
+    sizes = [int(x) for x in rng.choice([1024, 2048, 4096], 40, p=[0.3, 0.3, 0.4])]
+    polys = [O.seeded_fr(6000 + j, n) for j, n in enumerate(sizes)]
+    outs = [np.zeros((n // 8, 18), np.uint64) for n in sizes]
+    srv = engine.Server(served_ctx, max_rows=64, slots=2, hbm_budget=40 << 20)
+    tickets = [srv.submit(polys[j], outs[j]) for j in range(len(sizes))]
+    deadline = time.time() + 120
+    for t in tickets:
+        assert srv.wait(t, max(1, int(1000 * (deadline - time.time())))) == 0
+    st = srv.stats()
+    srv.close()
+    assert st["requests"] == len(sizes) and st["nomem"] == 0
+    assert st["packs"] >= 2 and st["mean_pack_rows"] < len(sizes)
+    for j, n in enumerate(sizes):
+        h = engine.empty((1, n // 8, 18))
+        served_ctx.poly2h_fft(h, engine.to_device(polys[j].reshape(1, n, 4)), 1, n)
+        assert np.array_equal(engine.to_host(h)[0], outs[j]), j
+
+
+def test_server_full_queue_refuses_with_eagain(engine, served_ctx):
+    """With max_queue requests waiting, submit refuses with FK20_EAGAIN (the
+    caller retries later) and counts the refusal; admitted requests are
+    proved exactly."""
+    srv = engine.Server(served_ctx, max_rows=1, slots=1, max_queue=4)
+    polys = [O.seeded_fr(7000 + j, 4096) for j in range(24)]
+    outs = [np.zeros((512, 18), np.uint64) for _ in polys]
+    admitted, refused = [], 0
+    for j in range(len(polys)):
+        try:
+            admitted.append((j, srv.submit(polys[j], outs[j])))
+        except engine.Fk20Error as e:
+            assert e.code == engine.FK20_EAGAIN
+            refused += 1
+    assert refused >= 1 and len(admitted) >= 4
+    deadline = time.time() + 120
+    for _, t in admitted:
+        assert srv.wait(t, max(1, int(1000 * (deadline - time.time())))) == 0
+    assert srv.stats()["rejected"] == refused
+    srv.close()
+    for j, _ in admitted[:3] + admitted[-1:]:
+        h = engine.empty((1, 512, 18))
+        served_ctx.poly2h_fft(h, engine.to_device(polys[j].reshape(1, 4096, 4)), 1, 4096)
+        assert np.array_equal(engine.to_host(h)[0], outs[j]), j

@@ -161,3 +161,60 @@ def test_fused_fft_schedule(emul, G, log_m):
             inv[m // 2:] = [0] * (m // 2)
             fwd = [sum(inv[j] * wp[(i * j) % m] for j in range(m)) % R for i in range(m)]
             assert vals[(k, g)] == fwd, (k, g)
+
+
+LAMBDA = 0xAC45A4010001A40200000000FFFFFFFF  # phi = [lambda] on G1, lambda^2 + lambda + 1 = r
+
+
+def program_partial_sums(prog):
+    """Replays a twiddle program (scalar_prog.cuh) on scalars mod r: yields,
+    before every mixed addition, (accumulator scalar, added point's scalar),
+    and returns the scalar of the result."""
+    r = O.R
+    hdr = int(prog[0])
+    assert not hdr & 0x300
+    top, acc, started, adds = hdr & 0xFF, 0, False, []
+    for pos in range(top, -1, -1):
+        if started:
+            acc = 2 * acc % r
+        byte = (int(prog[1 + (pos >> 2)]) >> ((pos & 3) * 8)) & 0xFF
+        for h in (0, 1):
+            code = (byte >> (4 * h)) & 15
+            if code & 1:
+                d = (2 * (code >> 2) + 1) * (-1 if code & 2 else 1)
+                q = d * (LAMBDA if h else 1) % r
+                if started:
+                    adds.append((acc, q))
+                    acc = (acc + q) % r
+                else:
+                    acc = q
+                started = True
+    if hdr & 0x400:
+        acc = -acc % r
+    return adds, acc
+
+
+def test_programs_avoid_the_mixed_additions_exceptional_cases(emul):
+    """The programs' main loop adds table points with the Jacobian mixed
+    addition, which is wrong when the accumulator equals the added point or
+    its negative, or is infinity.  For a point P of prime order r, acc = [a]P
+    and Q = [q]P, so this happens exactly when a = +-q or a = 0 (mod r): checked
+    here for every program the library builds (w^t, t < 512, w the 512th root
+    of unity of the twiddles, and 2^-s, s < 16), and each program's result is
+    its scalar."""
+    r = O.R
+    w = O.root_of_unity(512)
+    scalars = [pow(w, t, r) for t in range(512)] + [pow(pow(2, s, r), r - 2, r) for s in range(16)]
+    prog = np.zeros(64, np.uint32)
+    checked = 0
+    for k in scalars:
+        emul.emul_make_program(prog.ctypes.data_as(ctypes.c_void_p), P(O.int_to_limbs(k, 4)))
+        if int(prog[0]) & 0x300:  # 0 or +-1: no arithmetic
+            assert k in (1, r - 1)
+            continue
+        adds, res = program_partial_sums(prog)
+        assert res == k
+        for a, q in adds:
+            assert a != 0 and a != q and a != (r - q) % r, (hex(k), hex(a), hex(q))
+        checked += len(adds)
+    assert checked > 20000
