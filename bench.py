@@ -734,7 +734,8 @@ def ragged_on(ctx, rank, steps, warmup, ws=1):
 
 
 # ------------------------------------------------------------------ kernel microbenchmarks
-MP, MR = 300, 136  # limb products per Fp / Fr Montgomery product
+# limb products per Fp product (12-limb CIOS), Fp square (triangular), Fr product
+MP, MS, MR = 300, 234, 136
 
 
 def _timed(fn, reps, stream):
@@ -773,7 +774,7 @@ def run_micro(args, ws, rank, dev):
     # ---- field products: limb-major Montgomery data, `iters` dependent products per element
     count, iters = 1 << 24, 64
     rng = np.random.default_rng(3)
-    for field, mod, nl, mp in (("fp", P_MOD, 12, MP), ("fr", R_MOD, 8, MR)):
+    for field, mod, nl, mp, ms_ in (("fp", P_MOD, 12, MP, MS), ("fr", R_MOD, 8, MR, MR)):
         words = rng.integers(0, 2**32, (nl, count), dtype=np.uint64).astype(np.uint32)
         words[nl - 1] &= np.uint32((1 << (mod.bit_length() - 32 * (nl - 1) - 1)) - 1)  # < 2^(bits-1) < mod
         d0 = torch.from_numpy(words.view(np.int32)).cuda()
@@ -794,7 +795,7 @@ def run_micro(args, ws, rank, dev):
                 y = pow(x, 2 ** iters, mod) if sq else pow(x, iters + 1, mod)
                 G = sum(int(got[k, e]) << (32 * k) for k in range(nl))
                 ok &= G == y * Rm % mod
-            prod = count * iters * mp
+            prod = count * iters * (ms_ if sq else mp)
             out[f"{field}_{'sqr' if sq else 'mul'}"] = {
                 "elements": count, "products_per_element": iters, "ms": ms,
                 "gmul_per_s": count * iters / (ms * 1e-3) / 1e9,
@@ -809,9 +810,12 @@ def run_micro(args, ws, rank, dev):
     res = E.empty((rows, m, 18))
     costs = [E.program_cost(i) for i in range(512 + 10)]
 
-    def prog_products(idx):
+    def prog_products(idx):  # the engine's accounting of a twiddle program (scalar_prog.cuh)
         dbl, add = costs[idx]
-        return (dbl * 8 + add * 12 + 1) * MP if dbl or add else 0.0
+        if not (dbl or add):
+            return 0.0
+        return (6 * MP + 2 * MS) + 3 * 12 * MP + 30 * MP + MS + (dbl - 1) * (2 * MP + 5 * MS) + \
+            (add - 3) * (8 * MP + 3 * MS)
 
     def fft_products(inverse):
         tot = 0.0

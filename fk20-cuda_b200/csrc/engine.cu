@@ -357,20 +357,24 @@ struct DeviceGuard {  // make ctx->device current for the duration of a call
 };
 
 // ---- algorithmic work model (limb products) ----------------------------------
-// Fp products per operation: complete projective addition 12, doubling 8; the
-// MSM's mixed addition into an XYZZ accumulator 10 (8 M + 2 S)
-constexpr double MP = 300.0, MR = 136.0, ADD_P = 12 * MP, MADD_P = 10 * MP, DBL_P = 8 * MP;
+// An Fp product is 300 limb products (12-limb CIOS: 144 + 156), an Fp square
+// 234 (the triangular square: 78 + 156), an Fr product 136.  Per operation:
+// complete projective addition 12 M, doubling 6 M + 2 S; the MSM's mixed
+// addition into an XYZZ accumulator 8 M + 2 S.
+constexpr double MP = 300.0, MS = 234.0, MR = 136.0, ADD_P = 12 * MP, MADD_P = 8 * MP + 2 * MS,
+                 DBL_P = 6 * MP + 2 * MS;
 
 // A twiddle program (scalar_prog.cuh): 2P, 3P, 5P, 7P with the complete
-// projective formulas (1 doubling + 3 additions: 44), the four points made
-// affine on the isomorphic curve with their phi images (27) and the result
-// brought back (4), then Jacobian doublings of 7 and mixed additions of 11
-// for the digits (program_cost counts the precompute's doubling and three
-// additions with them).
+// projective formulas (1 doubling + 3 additions), the four points made affine
+// on the isomorphic curve with their phi images (27 M) and the result brought
+// back (3 M + 1 S), then Jacobian doublings (2 M + 5 S) and mixed additions
+// (8 M + 3 S) for the digits (program_cost counts the precompute's doubling
+// and three additions with them).
 double prog_products(int idx) {
     const HostConsts &hc = host_consts();
     if (hc.prog[idx][0] & 0x300u) return 0.0;
-    return (44.0 + 31.0 + 7.0 * (hc.prog_dbl[idx] - 1) + 11.0 * (hc.prog_add[idx] - 3)) * MP;
+    return DBL_P + 3 * ADD_P + 30.0 * MP + MS + (hc.prog_dbl[idx] - 1) * (2 * MP + 5 * MS) +
+           (hc.prog_add[idx] - 3) * (8 * MP + 3 * MS);
 }
 
 // one stage over `rows` rows: kind 0 DIF inverse, 1 DIT forward

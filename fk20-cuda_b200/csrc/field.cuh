@@ -85,6 +85,9 @@ template <class F> FK_D void ptx_row_odd(uint32_t *o, const uint32_t *a, uint32_
 template <class F> FK_D void ptx_red_even(uint32_t *e, uint32_t m);
 template <class F> FK_D void ptx_red_odd(uint32_t *o, uint32_t m);
 template <class F> FK_D void ptx_final(uint32_t *t, const uint32_t *e, const uint32_t *o);
+template <class F> FK_D void ptx_final_c(uint32_t *t, const uint32_t *e, const uint32_t *o, uint32_t c);
+template <class F, int I> FK_D void ptx_sqrow_even(uint32_t *e, const uint32_t *v, uint32_t b);
+template <class F, int I> FK_D void ptx_sqrow_odd(uint32_t *o, const uint32_t *v, uint32_t b);
 #if defined(__CUDA_ARCH__)
 #include "chains.inc"
 #endif
@@ -206,6 +209,52 @@ FK_HD void ch_final(uint32_t *t, const uint32_t *e, const uint32_t *o) {
 #endif
 }
 
+// t[0..N-1] = (e + o + c) >> 32 over N+1 words, c (0 or 1) added at word 0
+template <class F>
+FK_HD void ch_final_c(uint32_t *t, const uint32_t *e, const uint32_t *o, uint32_t c) {
+#if defined(__CUDA_ARCH__)
+    ptx_final_c<F>(t, e, o, c);
+#else
+    uint64_t s = ((uint64_t)e[0] + o[0] + c) >> 32;
+    for (int k = 1; k <= F::N; k++) {
+        s += (uint64_t)e[k] + o[k];
+        t[k - 1] = (uint32_t)s;
+        s >>= 32;
+    }
+#endif
+}
+
+// squaring row I >= 1, one parity P of j (0: the e half, 1: the o half):
+// acc[j0..] += v[j] * b for j >= I, j = P mod 2 (lo word at j, hi word at
+// j + 1), the carry out of the e half into e[N]; acc[N] is written, not read
+template <class F, int I, int P>
+FK_HD void ch_sqrow(uint32_t *acc, const uint32_t *v, uint32_t b) {
+#if defined(__CUDA_ARCH__)
+    if (P == 0) ptx_sqrow_even<F, I>(acc, v, b);
+    else ptx_sqrow_odd<F, I>(acc, v, b);
+#else
+    constexpr int N = F::N;
+    const int j0 = (I % 2 == P) ? I : I + 1;
+    if (j0 >= N) return;  // no product of this parity (acc[N] keeps its 0)
+    uint64_t c = 0;
+    for (int w = j0; w < N; w++) {
+        c += (uint64_t)acc[w] + (((w - j0) & 1) ? mul_hi(v[w - 1], b) : mul_lo(v[w], b));
+        acc[w] = (uint32_t)c;
+        c >>= 32;
+    }
+    acc[N] = P == 0 ? (uint32_t)c : (uint32_t)(c + mul_hi(v[N - 1], b));
+#endif
+}
+
+// the carry out of e0 + o0 + c, c = 0 or 1
+FK_HD uint32_t ch_carry3(uint32_t e0, uint32_t o0, uint32_t c) {
+#if defined(__CUDA_ARCH__)
+    return ptx_carry3(e0, o0, c);
+#else
+    return (uint32_t)(((uint64_t)e0 + o0 + c) >> 32);
+#endif
+}
+
 // the carry out of e0 + o0
 FK_HD uint32_t ch_carry0(uint32_t e0, uint32_t o0) {
 #if defined(__CUDA_ARCH__)
@@ -308,8 +357,84 @@ FK_HD void f_mul(Elem<F> &r, const Elem<F> &A, const Elem<F> &B) {
     f_reduce_once<F>(r.w, t);
 }
 
+// ---------------------------------------------------------------- Montgomery square
+// The same word-serial CIOS as f_mul, with the products of word i of A
+// restricted to words j >= i (78 of 144 limb products for Fp, 36 of 64 for
+// Fr): row i adds a_i * V_i, V_i = a_i 2^(32 i) + 2 sum_{j > i} a_j 2^(32 j),
+// whose words are a_i, a_{i+1} << 1 and then the words of 2A (the top bit of
+// a_i belongs to row i's own a_i, not to 2A's word i + 1).  Sum over i:
+// sum a_i^2 2^(64 i) + 2 sum_{i<j} a_i a_j 2^(32(i+j)) = A^2.  As a row no
+// longer starts at word 0, the word-0 carry c of each reduction step is
+// carried into the next step's word-0 sum (and the final shift) instead of
+// the odd half's first word.  Bounds: V_i <= 2A, so A < 2^(32N - 2) keeps
+// every partial value where f_mul's do (A canonical: A < m), except the top
+// word of the odd half, which holds hi(2 a_{N-1} a_i) + hi(m mod_{N-1}) and
+// stays below 2^32 only for a modulus whose top word is below 2^30 (Fp:
+// 0x1a0111ea; Fr's 0x73eda753 is not, so Fr squares are products).
+template <class F, int I>
+FK_HD void f_sqr_rows(uint32_t *e, uint32_t *o, uint32_t &c, const uint32_t *a, const uint32_t *a2) {
+    constexpr int N = F::N;
+    if constexpr (I > 0) {
+        uint32_t v[N];
+#pragma unroll
+        for (int j = 0; j < N; j++) v[j] = j == I ? a[I] : j == I + 1 ? a[I + 1] << 1 : a2[j];
+        ch_sqrow<F, I, 0>(e, v, a[I]);
+        ch_sqrow<F, I, 1>(o, v, a[I]);
+    }
+    // reduction: add m*p, m chosen so that word 0 (with the pending carry) vanishes
+    const uint32_t m = mul_lo(e[0] + o[0] + c, F::M0);
+    ch_red_even<F>(e, m);
+    ch_red_odd<F>(o, m);
+    if constexpr (I < N - 1) {
+        c = ch_carry3(e[0], o[0], c);
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            e[k] = e[k + 1];
+            o[k] = o[k + 1];
+        }
+        e[N] = 0;
+        o[N] = 0;
+        f_sqr_rows<F, I + 1>(e, o, c, a, a2);
+    }
+}
+
 template <class F>
-FK_HD void f_sqr(Elem<F> &r, const Elem<F> &a) { f_mul<F>(r, a, a); }
+FK_HD void f_sqr(Elem<F> &r, const Elem<F> &A) {
+    constexpr int N = F::N;
+    if constexpr (F::mod(N - 1) >= (1u << 30)) {
+        f_mul<F>(r, A, A);
+    } else {
+        const uint32_t *a = A.w;
+        uint32_t a2[N];  // the words of 2A
+        a2[0] = a[0] << 1;
+#pragma unroll
+        for (int j = 1; j < N; j++) a2[j] = (a[j] << 1) | (a[j - 1] >> 31);
+        uint32_t e[N + 1], o[N + 1];
+        uint32_t c = 0;
+        {
+            // row 0: V_0 = (a_0, a_1 << 1, 2A's words 2..N-1), plain products
+            const uint32_t b = a[0];
+#pragma unroll
+            for (int j = 0; j < N; j += 2) {
+                const uint32_t v = j == 0 ? a[0] : a2[j];
+                e[j] = mul_lo(v, b);
+                e[j + 1] = mul_hi(v, b);
+            }
+            e[N] = 0;
+            o[0] = 0;
+#pragma unroll
+            for (int j = 1; j < N; j += 2) {
+                const uint32_t v = j == 1 ? a[1] << 1 : a2[j];
+                o[j] = mul_lo(v, b);
+                o[j + 1] = mul_hi(v, b);
+            }
+        }
+        f_sqr_rows<F, 0>(e, o, c, a, a2);
+        uint32_t t[N];
+        ch_final_c<F>(t, e, o, c);
+        f_reduce_once<F>(r.w, t);
+    }
+}
 
 template <class F>
 FK_HD void f_add(Elem<F> &r, const Elem<F> &a, const Elem<F> &b) {

@@ -130,6 +130,55 @@ def gen(desc, n):
         lines.append("%s.u32 %s, %s, %s, %s" % ("madc.hi.cc" if k < half - 1 else "madc.hi", O(hi), m_, q_(k), O(hi)))
     out.append(block("ptx_red_odd", ("void", desc, "uint32_t *o, uint32_t m", "", ""), lines, outs, ins))
 
+    # squaring rows I = 1 .. n-1 (row 0 is plain products): e[j0..n-1] += v[j] * b
+    # for even j >= I (lo word at j, hi word at j + 1), e[n] = the carry out;
+    # o[j0..n] += v[j] * b for odd j >= I, o[n] written (its old value is 0)
+    for I in range(1, n):
+        for par, acc in ((0, "e"), (1, "o")):
+            js = [j for j in range(I, n) if j % 2 == par]
+            name = "ptx_sqrow_even" if par == 0 else "ptx_sqrow_odd"
+            sig = ("void", "%s, %d" % (desc, I), "uint32_t *%s, const uint32_t *v, uint32_t b" % acc, "", "")
+            if not js:
+                out.append("template <> FK_D void %s<%s, %d>(uint32_t *, const uint32_t *, uint32_t) {}\n" % (name, desc, I))
+                continue
+            j0 = js[0]
+            top = n if par == 0 else n + 1  # words j0 .. top - 1 are read and written
+            words = list(range(j0, top))
+            outs = []
+            for w in words:
+                last_even = par == 0 and w == n
+                outs.append('"%s"(%s[%d])' % ("=r" if (w == n) else "+r", acc, w))
+            if par == 0:
+                outs.append('"=r"(%s[%d])' % (acc, n))
+            op = {w: "%%%d" % k for k, w in enumerate(words + ([n] if par == 0 else []))}
+            base = len(outs)
+            ins = ['"r"(v[%d])' % j for j in js] + ['"r"(b)']
+            vj = {j: "%%%d" % (base + k) for k, j in enumerate(js)}
+            b_ = "%%%d" % (base + len(js))
+            lines = []
+            for k, j in enumerate(js):
+                lo, hi = j, j + 1
+                lines.append("%s.u32 %s, %s, %s, %s" % ("mad.lo.cc" if k == 0 else "madc.lo.cc", op[lo], vj[j], b_, op[lo]))
+                if hi == n and par == 1:
+                    lines.append("madc.hi.u32 %s, %s, %s, 0" % (op[hi], vj[j], b_))
+                else:
+                    lines.append("madc.hi.cc.u32 %s, %s, %s, %s" % (op[hi], vj[j], b_, op[hi]))
+            if par == 0:
+                lines.append("addc.u32 %s, 0, 0" % op[n])
+            out.append(block(name, sig, lines, outs, ins))
+
+    # t = (e + o + c) >> 32 over n + 1 words, c the pending word-0 carry (0 or 1)
+    outs = ['"=r"(t[%d])' % i for i in range(n)]
+    ins = ['"r"(e[%d])' % i for i in range(n + 1)] + ['"r"(o[%d])' % i for i in range(n + 1)] + ['"r"(c)']
+    E = lambda i: "%%%d" % (n + i)
+    Oo = lambda i: "%%%d" % (2 * n + 1 + i)
+    c_ = "%%%d" % (3 * n + 2)
+    lines = ["add.cc.u32 x, %s, -1" % c_, "addc.cc.u32 x, %s, %s" % (E(0), Oo(0))]
+    lines += ["addc.cc.u32 %%%d, %s, %s" % (k - 1, E(k), Oo(k)) for k in range(1, n)]
+    lines += ["addc.u32 %%%d, %s, %s" % (n - 1, E(n), Oo(n))]
+    out.append(block("ptx_final_c", ("void", desc, "uint32_t *t, const uint32_t *e, const uint32_t *o, uint32_t c", "", ""),
+                     lines, outs, ins, temps=("x",)))
+
     # t = (e + o) >> 32 over n + 1 words
     outs = ['"=r"(t[%d])' % i for i in range(n)]
     ins = ['"r"(e[%d])' % i for i in range(n + 1)] + ['"r"(o[%d])' % i for i in range(n + 1)]
@@ -163,6 +212,20 @@ def main():
     print('        : "=r"(c)')
     print('        : "r"(e0), "r"(o0));')
     print("    return c;")
+    print("}")
+    # carry out of e0 + o0 + c (c = 0 or 1): the carry flag is set to c first
+    print("// the carry out of e0 + o0 + c, c = 0 or 1")
+    print("FK_D uint32_t ptx_carry3(uint32_t e0, uint32_t o0, uint32_t c) {")
+    print("    uint32_t r;")
+    print('    asm volatile("{\\n\\t"')
+    print('        ".reg .u32 x;\\n\\t"')
+    print('        "add.cc.u32 x, %3, -1;\\n\\t"')
+    print('        "addc.cc.u32 x, %1, %2;\\n\\t"')
+    print('        "addc.u32 %0, 0, 0;\\n\\t"')
+    print('        "}"')
+    print('        : "=r"(r)')
+    print('        : "r"(e0), "r"(o0), "r"(c));')
+    print("    return r;")
     print("}")
     print("// clang-format on")
 

@@ -39,37 +39,41 @@ FK_D void f2_xi(Fp2 &r, const Fp2 &a) {
     f_add(r.c1, a.c0, a.c1);
     r.c0 = t;
 }
-// 3 Fp products; r may alias a or b
-static __device__ __noinline__ void f2_mul(Fp2 *r, const Fp2 *a, const Fp2 *b) {
+// 3 Fp products.  The out-of-line Fp2 routines take and return values, not
+// pointers: with pointer arguments (r may alias a or b) some code
+// arrangements of their callers -- an Fp6 sum as a rolled loop before an
+// in-place product by a line -- gave wrong values in the GPU build while the
+// source is right (it is right on the host and unoptimised); with values they
+// give the right ones in every arrangement tried (tests/host/tower_probe.cu).
+static __device__ __noinline__ Fp2 f2_mul_v(Fp2 a, Fp2 b) {
     Fp t0, t1, s0, s1;
-    fp_mul(t0, a->c0, b->c0);
-    fp_mul(t1, a->c1, b->c1);
-    f_add(s0, a->c0, a->c1);
-    f_add(s1, b->c0, b->c1);
+    Fp2 r;
+    fp_mul(t0, a.c0, b.c0);
+    fp_mul(t1, a.c1, b.c1);
+    f_add(s0, a.c0, a.c1);
+    f_add(s1, b.c0, b.c1);
     fp_mul(s0, s0, s1);
     f_sub(s0, s0, t0);
-    f_sub(r->c1, s0, t1);
-    f_sub(r->c0, t0, t1);
+    f_sub(r.c1, s0, t1);
+    f_sub(r.c0, t0, t1);
+    return r;
 }
 // (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
-static __device__ __noinline__ void f2_sqr(Fp2 *r, const Fp2 *a) {
+static __device__ __noinline__ Fp2 f2_sqr_v(Fp2 a) {
     Fp s, d, t;
-    f_add(s, a->c0, a->c1);
-    f_sub(d, a->c0, a->c1);
-    fp_mul(t, a->c0, a->c1);
-    fp_mul(r->c0, s, d);
-    f_add(r->c1, t, t);
-}
-FK_D Fp2 f2m(const Fp2 &a, const Fp2 &b) {
     Fp2 r;
-    f2_mul(&r, &a, &b);
+    f_add(s, a.c0, a.c1);
+    f_sub(d, a.c0, a.c1);
+    fp_mul(t, a.c0, a.c1);
+    fp_mul(r.c0, s, d);
+    f_add(r.c1, t, t);
     return r;
 }
-FK_D Fp2 f2s(const Fp2 &a) {
-    Fp2 r;
-    f2_sqr(&r, &a);
-    return r;
-}
+// r may alias a or b
+FK_D void f2_mul(Fp2 *r, const Fp2 *a, const Fp2 *b) { *r = f2_mul_v(*a, *b); }
+FK_D void f2_sqr(Fp2 *r, const Fp2 *a) { *r = f2_sqr_v(*a); }
+FK_D Fp2 f2m(const Fp2 &a, const Fp2 &b) { return f2_mul_v(a, b); }
+FK_D Fp2 f2s(const Fp2 &a) { return f2_sqr_v(a); }
 FK_D void f2_mul_fp(Fp2 &r, const Fp2 &a, const Fp &s) {
     fp_mul(r.c0, a.c0, s);
     fp_mul(r.c1, a.c1, s);
