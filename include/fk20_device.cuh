@@ -10,13 +10,26 @@
  *  - g1p_t is homogeneous projective (x = X/Z, y = Y/Z); any (0, y != 0, 0)
  *    is the point at infinity (G1P_ANYINF), written as (0, 1, 0).
  *
- * Each call converts its operands into the engine's Montgomery form, runs the
- * engine's arithmetic (field.cuh, g1.cuh: CIOS products, RCB complete
- * formulas) and converts the result back, so it costs about one extra
- * product per operand; the batched host entry points and the FK20 pipeline
- * keep values in Montgomery form throughout.  The block-level fr_fft /
- * fr_ift / g1p_fft / g1p_ift device functions of the reference are provided
- * as host launchers in fk20_b200.h instead.
+ * Cost model.  Words are only reduced on the way in (conditional subtractions
+ * of 8p, 4p, 2p, p -- or 2r, r -- so any 384-/256-bit representative is
+ * accepted) and the engine's Montgomery arithmetic runs on the standard-form
+ * words directly:
+ *  - additions, subtractions, negation, x2..x12, comparisons: no products;
+ *  - fp_mul / fr_mul / squares: MontMul(x, y) = x y R^-1, then one more
+ *    Montgomery product by R^2 mod p restores x y -- two products where a
+ *    convert-in / multiply / convert-out wrapper needs four;
+ *  - G1: homogeneous projective coordinates are defined up to a common
+ *    non-zero factor, and standard-form words (X, Y, Z) read as Montgomery
+ *    values are (X, Y, Z) R^-1 -- the same point.  The engine's complete
+ *    formulas (whose only constant, b3 = 12, is applied by additions) therefore
+ *    run on the words as they are, with no conversion.  A g1p_t result is the
+ *    reference's point, but its coordinates may differ from the reference's by
+ *    a common factor (a power of R): compare with g1p_eq, or normalise with
+ *    g1a_fromG1p, as the reference's own tests do (g1p_compare.cu:23).
+ * The batched host entry points and the FK20 pipeline keep values in
+ * Montgomery form throughout.  The block-level fr_fft / fr_ift / g1p_fft /
+ * g1p_ift device functions of the reference are provided as host launchers
+ * in fk20_b200.h instead.
  *
  * Use: nvcc -gencode arch=compute_100a,code=sm_100a -I include ... with this
  * repository's layout (the header includes ../fk20-cuda_b200/csrc/).
@@ -44,17 +57,55 @@ __device__ __forceinline__ void store_words(uint64_t (&x)[W], const Elem<F> &e) 
 #pragma unroll
     for (int k = 0; k < W; k++) x[k] = (uint64_t)e.w[2 * k] | ((uint64_t)e.w[2 * k + 1] << 32);
 }
-// standard form (any representative) -> Montgomery form, canonical
-__device__ __forceinline__ void mont(Fp &m, const fp_t &x) { Fp t; load_words(t, x); f_to_mont(m, t); }
-__device__ __forceinline__ void mont(Fr &m, const fr_t &x) { Fr t; load_words(t, x); f_to_mont(m, t); }
+// e mod m for any e < 2^(32N): subtract 2^k m where it fits, k = K..0.  Fp:
+// 2^384 < 10 p, so K = 3 (8p < 2^384); Fr: 2^256 < 3 r, so K = 1.
+template <class F, int K>
+__device__ __forceinline__ void reduce_any(Elem<F> &e) {
+#pragma unroll
+    for (int k = K; k >= 0; k--) {
+        uint32_t m[F::N], t[F::N];
+#pragma unroll
+        for (int i = 0; i < F::N; i++) m[i] = (F::mod(i) << k) | (i > 0 && k > 0 ? F::mod(i - 1) >> (32 - k) : 0u);
+        const uint32_t borrow = ch_sub<F>(t, e.w, m);  // all ones when e < 2^k m
+#pragma unroll
+        for (int i = 0; i < F::N; i++) e.w[i] = (e.w[i] & borrow) | (t[i] & ~borrow);
+    }
+}
+// any standard-form representative -> canonical standard form (no products)
+__device__ __forceinline__ void canon(Fp &e, const fp_t &x) { load_words(e, x); reduce_any<FpDesc, 3>(e); }
+__device__ __forceinline__ void canon(Fr &e, const fr_t &x) { load_words(e, x); reduce_any<FrDesc, 1>(e); }
+// standard-form product of canonical a, b: MontMul(R^2, MontMul(a, b)) = a b
+template <class F>
+__device__ __forceinline__ void std_mul(Elem<F> &r, const Elem<F> &a, const Elem<F> &b) {
+    Elem<F> t;
+    f_mul(t, a, b);
+    f_to_mont(r, t);
+}
+template <class F>
+__device__ __forceinline__ void std_sqr(Elem<F> &r, const Elem<F> &a) {
+    Elem<F> t;
+    f_sqr(t, a);
+    f_to_mont(r, t);
+}
+// standard-form inverse of canonical a: f_inv reads a as the Montgomery form
+// of a R^-1 and returns the words of a^-1 R^2; two Montgomery products by 1
+// take off R^2 (inv(0) = 0)
+template <class F>
+__device__ __forceinline__ void std_inv(Elem<F> &r, const Elem<F> &a) {
+    Elem<F> t;
+    f_inv(t, a);
+    f_from_mont(t, t);
+    f_from_mont(r, t);
+}
 // Montgomery form -> canonical standard form
 __device__ __forceinline__ void plain(fp_t &z, const Fp &m) { Fp t; f_from_mont(t, m); store_words(z, t); }
-__device__ __forceinline__ void plain(fr_t &z, const Fr &m) { Fr t; f_from_mont(t, m); store_words(z, t); }
 
+// a g1p_t as engine coordinates: canonical words, no conversion (the same
+// projective point, see the header comment); any (0, y != 0, 0) -> infinity
 __device__ __forceinline__ void point(G1P &p, const g1p_t &q) {
-    mont(p.x, q.x);
-    mont(p.y, q.y);
-    mont(p.z, q.z);
+    canon(p.x, q.x);
+    canon(p.y, q.y);
+    canon(p.z, q.z);
     if (f_is_zero(p.z)) g1_set_inf(p);
 }
 __device__ __forceinline__ void unpoint(g1p_t &q, const G1P &p) {
@@ -64,15 +115,18 @@ __device__ __forceinline__ void unpoint(g1p_t &q, const G1P &p) {
         q.y[0] = 1;
         return;
     }
-    plain(q.x, p.x);
-    plain(q.y, p.y);
-    plain(q.z, p.z);
+    store_words(q.x, p.x);
+    store_words(q.y, p.y);
+    store_words(q.z, p.z);
 }
-// affine (x, y); (0, 0) is the point at infinity
+// affine (x, y) -> (x : y : 1) with Z the standard-form word 1 (the Montgomery
+// one would give the point (x R^-1 : y R^-1 : 1), another point); (0, 0) is
+// the point at infinity
 __device__ __forceinline__ void point(G1P &p, const g1a_t &a) {
-    mont(p.x, a.x);
-    mont(p.y, a.y);
-    f_set_one(p.z);
+    canon(p.x, a.x);
+    canon(p.y, a.y);
+    f_set_zero(p.z);
+    p.z.w[0] = 1;
     if (f_is_zero(p.x) && f_is_zero(p.y)) g1_set_inf(p);
 }
 }  // namespace fk20_device_detail
@@ -88,9 +142,9 @@ __device__ __host__ inline void fp_one(fp_t &z) { fp_zero(z); z[0] = 1; }
     __device__ inline void name(fp_t &z, const fp_t &x) {     \
         using namespace fk20_device_detail;                   \
         fk::Fp a, r;                                          \
-        mont(a, x);                                           \
+        canon(a, x);                                          \
         body;                                                 \
-        plain(z, r);                                          \
+        store_words(z, r);                                    \
     }
 FK20_DEV_FP_UNARY(fp_neg, fk::f_neg(r, a))
 FK20_DEV_FP_UNARY(fp_x2, fk::f_add(r, a, a))
@@ -98,65 +152,67 @@ FK20_DEV_FP_UNARY(fp_x3, { fk::f_add(r, a, a); fk::f_add(r, r, a); })
 FK20_DEV_FP_UNARY(fp_x4, { fk::f_add(r, a, a); fk::f_add(r, r, r); })
 FK20_DEV_FP_UNARY(fp_x8, { fk::f_add(r, a, a); fk::f_add(r, r, r); fk::f_add(r, r, r); })
 FK20_DEV_FP_UNARY(fp_x12, fk::f_mul12(r, a))
-FK20_DEV_FP_UNARY(fp_sqr, fk::f_mul(r, a, a))
-FK20_DEV_FP_UNARY(fp_inv, fk::f_inv(r, a))
+FK20_DEV_FP_UNARY(fp_sqr, std_sqr(r, a))
+FK20_DEV_FP_UNARY(fp_inv, std_inv(r, a))
 #undef FK20_DEV_FP_UNARY
 
 __device__ inline void fp_reduce6(fp_t &z) {
     using namespace fk20_device_detail;
     fk::Fp a;
-    mont(a, z);
-    plain(z, a);
+    canon(a, z);
+    store_words(z, a);
 }
 __device__ inline void fp_add(fp_t &z, const fp_t &x, const fp_t &y) {
     using namespace fk20_device_detail;
     fk::Fp a, b;
-    mont(a, x);
-    mont(b, y);
+    canon(a, x);
+    canon(b, y);
     fk::f_add(a, a, b);
-    plain(z, a);
+    store_words(z, a);
 }
 __device__ inline void fp_sub(fp_t &z, const fp_t &x, const fp_t &y) {
     using namespace fk20_device_detail;
     fk::Fp a, b;
-    mont(a, x);
-    mont(b, y);
+    canon(a, x);
+    canon(b, y);
     fk::f_sub(a, a, b);
-    plain(z, a);
+    store_words(z, a);
 }
 __device__ inline void fp_mul(fp_t &z, const fp_t &x, const fp_t &y) {
     using namespace fk20_device_detail;
     fk::Fp a, b;
-    mont(a, x);
-    mont(b, y);
-    fk::f_mul(a, a, b);
-    plain(z, a);
+    canon(a, x);
+    canon(b, y);
+    std_mul(a, a, b);
+    store_words(z, a);
 }
-// z = v w + x y (fp_mma.cu:21)
+// z = v w + x y (fp_mma.cu:21): MontMul(v, w) + MontMul(x, y) = (v w + x y) R^-1,
+// then one product by R^2 -- three products
 __device__ inline void fp_mma(fp_t &z, const fp_t &v, const fp_t &w, const fp_t &x, const fp_t &y) {
     using namespace fk20_device_detail;
     fk::Fp a, b, c, d;
-    mont(a, v);
-    mont(b, w);
-    mont(c, x);
-    mont(d, y);
+    canon(a, v);
+    canon(b, w);
+    canon(c, x);
+    canon(d, y);
     fk::f_mul(a, a, b);
     fk::f_mul(c, c, d);
     fk::f_add(a, a, c);
-    plain(z, a);
+    fk::f_to_mont(a, a);
+    store_words(z, a);
 }
 __device__ inline bool fp_eq(const fp_t &x, const fp_t &y) {
     using namespace fk20_device_detail;
     fk::Fp a, b;
-    mont(a, x);
-    mont(b, y);
+    canon(a, x);
+    canon(b, y);
     return fk::f_eq(a, b);
 }
 __device__ inline bool fp_neq(const fp_t &x, const fp_t &y) { return !fp_eq(x, y); }
 __device__ inline bool fp_iszero(const fp_t &x) {
     using namespace fk20_device_detail;
     fk::Fp a;
-    mont(a, x);
+    canon(a, x);
     return fk::f_is_zero(a);
 }
 __device__ inline bool fp_nonzero(const fp_t &x) { return !fp_iszero(x); }
@@ -181,9 +237,9 @@ __device__ __host__ inline void fr_one(fr_t &z) { fr_zero(z); z[0] = 1; }
     __device__ inline void name(fr_t &z) {                    \
         using namespace fk20_device_detail;                   \
         fk::Fr a, r;                                          \
-        mont(a, z);                                           \
+        canon(a, z);                                          \
         body;                                                 \
-        plain(z, r);                                          \
+        store_words(z, r);                                    \
     }
 FK20_DEV_FR_INPLACE(fr_reduce4, r = a)
 FK20_DEV_FR_INPLACE(fr_neg, fk::f_neg(r, a))
@@ -192,47 +248,47 @@ FK20_DEV_FR_INPLACE(fr_x3, { fk::f_add(r, a, a); fk::f_add(r, r, a); })
 FK20_DEV_FR_INPLACE(fr_x4, { fk::f_add(r, a, a); fk::f_add(r, r, r); })
 FK20_DEV_FR_INPLACE(fr_x8, { fk::f_add(r, a, a); fk::f_add(r, r, r); fk::f_add(r, r, r); })
 FK20_DEV_FR_INPLACE(fr_x12, fk::f_mul12(r, a))
-FK20_DEV_FR_INPLACE(fr_sqr, fk::f_mul(r, a, a))
-FK20_DEV_FR_INPLACE(fr_inv, fk::f_inv(r, a))
+FK20_DEV_FR_INPLACE(fr_sqr, std_sqr(r, a))
+FK20_DEV_FR_INPLACE(fr_inv, std_inv(r, a))
 #undef FK20_DEV_FR_INPLACE
 
 #define FK20_DEV_FR_BINARY(name, op)                          \
     __device__ inline void name(fr_t &z, const fr_t &x) {     \
         using namespace fk20_device_detail;                   \
         fk::Fr a, b;                                          \
-        mont(a, z);                                           \
-        mont(b, x);                                           \
+        canon(a, z);                                          \
+        canon(b, x);                                          \
         op(a, a, b);                                          \
-        plain(z, a);                                          \
+        store_words(z, a);                                    \
     }
 FK20_DEV_FR_BINARY(fr_add, fk::f_add)
 FK20_DEV_FR_BINARY(fr_sub, fk::f_sub)
-FK20_DEV_FR_BINARY(fr_mul, fk::f_mul)
+FK20_DEV_FR_BINARY(fr_mul, std_mul)
 #undef FK20_DEV_FR_BINARY
 
 // (x, y) <- (x + y, x - y)   (fr_addsub.cu:18)
 __device__ inline void fr_addsub(fr_t &x, fr_t &y) {
     using namespace fk20_device_detail;
     fk::Fr a, b, s, d;
-    mont(a, x);
-    mont(b, y);
+    canon(a, x);
+    canon(b, y);
     fk::f_add(s, a, b);
     fk::f_sub(d, a, b);
-    plain(x, s);
-    plain(y, d);
+    store_words(x, s);
+    store_words(y, d);
 }
 __device__ inline bool fr_eq(const fr_t &x, const fr_t &y) {
     using namespace fk20_device_detail;
     fk::Fr a, b;
-    mont(a, x);
-    mont(b, y);
+    canon(a, x);
+    canon(b, y);
     return fk::f_eq(a, b);
 }
 __device__ inline bool fr_neq(const fr_t &x, const fr_t &y) { return !fr_eq(x, y); }
 __device__ inline bool fr_iszero(const fr_t &x) {
     using namespace fk20_device_detail;
     fk::Fr a;
-    mont(a, x);
+    canon(a, x);
     return fk::f_is_zero(a);
 }
 __device__ inline bool fr_nonzero(const fr_t &x) { return !fr_iszero(x); }
@@ -324,13 +380,14 @@ __device__ inline bool g1p_neq(const g1p_t &p, const g1p_t &q) { return !g1p_eq(
 __device__ inline bool g1p_isInf(const g1p_t &p) {
     return fp_iszero(p.z) && fp_iszero(p.x) && fp_nonzero(p.y);
 }
-// Y^2 Z == X^3 + 4 Z^3, or infinity (g1p_ispoint.cu:14-60)
+// Y^2 Z == X^3 + 4 Z^3, or infinity (g1p_ispoint.cu:14-60); homogeneous, so
+// the words may be read as Montgomery values (both sides scale by R^-3)
 __device__ inline bool g1p_isPoint(const g1p_t &p) {
     using namespace fk20_device_detail;
     fk::Fp x, y, z;
-    mont(x, p.x);
-    mont(y, p.y);
-    mont(z, p.z);
+    canon(x, p.x);
+    canon(y, p.y);
+    canon(z, p.z);
     if (fk::f_is_zero(z)) return fk::f_is_zero(x) && !fk::f_is_zero(y);
     fk::Fp l, r, t;
     fk::f_mul(l, y, y);

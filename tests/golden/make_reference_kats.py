@@ -19,7 +19,7 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FK20_REFERENCE", "/root/reference")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 ROW = re.compile(r"\{\s*((?:0x[0-9a-fA-F]+\s*,\s*)*0x[0-9a-fA-F]+)\s*,?\s*\}")

@@ -74,3 +74,44 @@ extern "C" int devapi_g1(int op, void *z, const void *x, const void *y, const vo
     k_g1<<<(n + 63) / 64, 64>>>(op, (g1p_t *)z, (const g1p_t *)x, (const g1p_t *)y, (const fr_t *)s, n);
     return (int)cudaDeviceSynchronize();
 }
+
+// Throughput of a dependent chain of standard-form products, `iters` per
+// element: form 0 is fp_mul of the device API (two Montgomery products);
+// form 1 converts both operands in, multiplies and converts back (four),
+// the wrapper the API's cost is compared against.
+__device__ __forceinline__ void fp_mul_convert(fp_t &z, const fp_t &x, const fp_t &y) {
+    using namespace fk20_device_detail;
+    fk::Fp a, b, t;
+    load_words(t, x);
+    fk::f_to_mont(a, t);
+    load_words(t, y);
+    fk::f_to_mont(b, t);
+    fk::f_mul(a, a, b);
+    plain(z, a);
+}
+__global__ void k_fp_rate(int form, fp_t *x, const fp_t *y, int n, int iters) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    fp_t a, b;
+    fp_cpy(a, x[i]);
+    fp_cpy(b, y[i]);
+    if (form == 0)
+        for (int k = 0; k < iters; k++) fp_mul(a, a, b);
+    else
+        for (int k = 0; k < iters; k++) fp_mul_convert(a, a, b);
+    fp_cpy(x[i], a);
+}
+extern "C" int devapi_fp_rate(int form, void *x, const void *y, int n, int iters, float *ms) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    k_fp_rate<<<(n + 127) / 128, 128>>>(form, (fp_t *)x, (const fp_t *)y, n, 1);  // warm-up
+    cudaEventRecord(e0);
+    k_fp_rate<<<(n + 127) / 128, 128>>>(form, (fp_t *)x, (const fp_t *)y, n, iters);
+    cudaEventRecord(e1);
+    const int rc = (int)cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc ? rc : (int)cudaGetLastError();
+}

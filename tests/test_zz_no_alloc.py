@@ -54,3 +54,22 @@ def test_noalloc_fft_rejects_requests_beyond_its_scratch(engine):
     rc = lib.g1p_fft_noalloc(engine._ptr(out), engine._ptr(pts), 9, 65, 0, engine._stream())
     assert rc == engine.FK20_ETOOBIG
     assert lib.g1p_fft_noalloc(engine._ptr(out), engine._ptr(pts), 10, 1, 0, engine._stream()) == engine.FK20_EINVAL
+
+
+def test_noalloc_fft_matches_oracle(engine):
+    """Independent of the allocating entry point: the oracle's G1 FFT
+    (the reference's g1p_fft / g1p_ift, g1p_fft.cu:337-350) on a few small
+    transforms, forward and inverse, compared after affine normalisation."""
+    import torch
+    lib = engine.lib()
+    st = engine._stream()
+    for log_m, count, inverse, seed in ((4, 3, 0, 21), (5, 2, 1, 22)):
+        m = 1 << log_m
+        pts = subgroup_points(engine, seed, count * m).reshape(count, m, 18)
+        got = engine.empty((count, m, 18))
+        assert lib.g1p_fft_noalloc(engine._ptr(got), engine._ptr(pts), log_m, count, inverse, st) == 0
+        torch.cuda.synchronize()
+        host_in = engine.to_host(pts)
+        exp = np.stack([O.g1_fft(host_in[k], inverse=bool(inverse)) for k in range(count)])
+        norm = lambda a: O.g1_normalize(np.ascontiguousarray(a).reshape(-1, 18)).reshape(count, m, 18)
+        assert np.array_equal(norm(engine.to_host(got)), norm(exp)), (log_m, count, inverse)
