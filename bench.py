@@ -611,6 +611,9 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
                       "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
                       "max_ms": st["max_ms"], "p99_below_plain_batch_latency": st["p99_ms"] < plain_ms,
                       "mean_pack_rows": st["mean_pack_rows"], "packs": st["packs"],
+                      # where the latency goes: waiting for a pack, staging it, running it
+                      "mean_wait_ms": st["mean_wait_ms"], "mean_enqueue_ms": st["mean_enqueue_ms"],
+                      "mean_run_ms": st["mean_run_ms"],
                       "errors": sum(1 for r in done_rc if r != 0),
                       # the load generator itself: requests/s it achieved against the schedule's
                       "arrivals_per_s": {"offered": rate, "achieved": count / submit_s},

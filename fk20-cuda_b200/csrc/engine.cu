@@ -1606,6 +1606,7 @@ struct Slot {
     std::vector<Req> reqs;     // the pack in flight (empty: the slot is free)
     std::vector<size_t> out_at;  // g1p_t offset of each request's proofs in hout
     int rc = 0;                // error of enqueueing the pack
+    Clock::time_point t_form, t_enq;  // the pack was formed / fully enqueued
     size_t bytes() const { return ws.bytes() + dpoly.bytes + dout.bytes; }
 };
 
@@ -1653,6 +1654,7 @@ struct fk20_server {
     // statistics since the last reset
     std::vector<double> lat_ms;
     uint64_t proofs = 0, packs = 0, pack_rows = 0, rejected = 0, nomem = 0;
+    double sum_wait_ms = 0, sum_enqueue_ms = 0, sum_run_ms = 0;  // where the latency goes
     Clock::time_point first, last;
     bool started = false;
 };
@@ -1751,6 +1753,7 @@ void server_main(fk20_server *s) {
             }
             s->packs++;
             s->pack_rows += done.size();
+            s->sum_run_ms += std::chrono::duration<double, std::milli>(now - sl.t_enq).count();
             s->last = now;
             sl.rc = 0;
             retired = true;
@@ -1777,25 +1780,34 @@ void server_main(fk20_server *s) {
             // Admission by device memory: the packs in flight and this one stay
             // within the budget, and whatever this pack adds to its slot's
             // buffers must be free on the device now (less a reserve for the
-            // runtime and other users of the GPU).
+            // runtime and other users of the GPU).  A pack that fits the
+            // slot's buffers takes no new memory, so the device is only asked
+            // (once, without holding the server lock: submit must not wait on
+            // the driver) when a pack would grow them.
             size_t limit = s->cfg.hbm_budget;
-            {
-                size_t fr = 0, tot = 0;
-                if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
-                    const size_t reserve = (size_t)256 << 20;
-                    limit = std::min(limit, others + fs->bytes() + (fr > reserve ? fr - reserve : 0));
-                } else {
-                    cudaGetLastError();
-                }
-            }
+            bool asked = false;
             unsigned cnt[3] = {0, 0, 0};
             size_t q = 0;
             for (; q < s->queue.size() && fs->reqs.size() < cap; q++) {
-                const Req &r = s->queue[q];
+                const Req r = s->queue[q];
                 const int k = log_m_for_n(r.n) - 7;
                 unsigned c2[3] = {cnt[0], cnt[1], cnt[2]};
                 c2[k]++;
-                if (others + std::max(fs->bytes(), pack_bytes(c2)) > limit) break;
+                const size_t need = std::max(fs->bytes(), pack_bytes(c2));
+                if (need > fs->bytes() && !asked) {
+                    asked = true;
+                    size_t fr = 0, tot = 0;
+                    lk.unlock();  // producers only append to the queue; the worker alone removes
+                    const cudaError_t e = cudaMemGetInfo(&fr, &tot);
+                    lk.lock();
+                    if (e == cudaSuccess) {
+                        const size_t reserve = (size_t)256 << 20;
+                        limit = std::min(limit, others + fs->bytes() + (fr > reserve ? fr - reserve : 0));
+                    } else {
+                        cudaGetLastError();
+                    }
+                }
+                if (others + need > limit) break;
                 cnt[k]++;
                 fs->reqs.push_back(r);
             }
@@ -1832,9 +1844,14 @@ void server_main(fk20_server *s) {
                 }
                 continue;
             } else {
+                fs->t_form = Clock::now();
+                for (const Req &r : fs->reqs)
+                    s->sum_wait_ms += std::chrono::duration<double, std::milli>(fs->t_form - r.t0).count();
                 lk.unlock();
                 fs->rc = enqueue_pack(s, *fs, latency);
+                fs->t_enq = Clock::now();
                 lk.lock();
+                s->sum_enqueue_ms += std::chrono::duration<double, std::milli>(fs->t_enq - fs->t_form).count();
                 continue;
             }
         }
@@ -2004,6 +2021,9 @@ int fk20_server_get_stats(fk20_server *s, fk20_server_stats *out) {
     st.mean_pack_rows = s->packs ? (double)s->pack_rows / s->packs : 0;
     st.rejected = s->rejected;
     st.nomem = s->nomem;
+    st.mean_wait_ms = v.empty() ? 0 : s->sum_wait_ms / v.size();
+    st.mean_enqueue_ms = s->packs ? s->sum_enqueue_ms / s->packs : 0;
+    st.mean_run_ms = s->packs ? s->sum_run_ms / s->packs : 0;
     *out = st;
     return 0;
 }
@@ -2013,6 +2033,7 @@ int fk20_server_reset_stats(fk20_server *s) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->lat_ms.clear();
     s->proofs = s->packs = s->pack_rows = s->rejected = s->nomem = 0;
+    s->sum_wait_ms = s->sum_enqueue_ms = s->sum_run_ms = 0;
     s->started = false;
     return 0;
 }

@@ -72,7 +72,9 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("requests", ctypes.c_uint64), ("proofs", ctypes.c_uint64), ("packs", ctypes.c_uint64),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
                 ("max_ms", ctypes.c_double), ("wall_s", ctypes.c_double), ("proofs_per_s", ctypes.c_double),
-                ("mean_pack_rows", ctypes.c_double), ("rejected", ctypes.c_uint64), ("nomem", ctypes.c_uint64)]
+                ("mean_pack_rows", ctypes.c_double), ("rejected", ctypes.c_uint64), ("nomem", ctypes.c_uint64),
+                ("mean_wait_ms", ctypes.c_double), ("mean_enqueue_ms", ctypes.c_double),
+                ("mean_run_ms", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -294,6 +294,9 @@ typedef struct {
     double mean_pack_rows;
     uint64_t rejected; /* submits refused with FK20_EAGAIN (max_queue requests waiting) */
     uint64_t nomem;    /* requests failed with FK20_ENOMEM (too large for the device memory alone) */
+    double mean_wait_ms;    /* submit -> the request's pack is formed (mean over requests) */
+    double mean_enqueue_ms; /* host time to stage and enqueue a pack (mean over packs) */
+    double mean_run_ms;     /* pack enqueued -> its proofs copied out (mean over packs) */
 } fk20_server_stats;
 int fk20_server_create(fk20_server **srv, fk20_ctx *ctx, const fk20_server_config *cfg);
 /* poly: HOST array of n fr_t (n in 1024, 2048, 4096); h_fft: HOST array of

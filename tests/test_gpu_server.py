@@ -101,15 +101,17 @@ def test_server_close_finishes_pending_requests(engine, served_ctx):
 
 
 def test_server_memory_budget_limits_packs(engine, served_ctx):
-    """Admission by device memory: with a budget of 40 MiB for both slots'
-    buffers (a 4096-coefficient request needs ~10 MiB of tiles for its 32-row
-    group), the 40 requests submitted at once cannot form one pack; they are
-    proved in several, every one of them exact."""
+    """Admission by device memory: with a budget of 20 MiB for both slots'
+    buffers, the 40 requests submitted at once cannot form one pack (a pack
+    of all three lengths needs ~19 MB of scalar and point tiles -- 10.7, 5.4
+    and 2.7 MB for the 32-row groups of 4096, 2048 and 1024 coefficients --
+    plus ~5 MB of staged inputs and outputs); they are proved in several,
+    every one of them exact."""
     rng = np.random.default_rng(8)
     sizes = [int(x) for x in rng.choice([1024, 2048, 4096], 40, p=[0.3, 0.3, 0.4])]
     polys = [O.seeded_fr(6000 + j, n) for j, n in enumerate(sizes)]
     outs = [np.zeros((n // 8, 18), np.uint64) for n in sizes]
-    srv = engine.Server(served_ctx, max_rows=64, slots=2, hbm_budget=40 << 20)
+    srv = engine.Server(served_ctx, max_rows=64, slots=2, hbm_budget=20 << 20)
     tickets = [srv.submit(polys[j], outs[j]) for j in range(len(sizes))]
     deadline = time.time() + 120
     for t in tickets:
