@@ -817,8 +817,7 @@ def run_micro(args, ws, rank, dev):
         dbl, add = costs[idx]
         if not (dbl or add):
             return 0.0
-        return (6 * MP + 2 * MS) + 3 * 12 * MP + 30 * MP + MS + (dbl - 1) * (2 * MP + 5 * MS) + \
-            (add - 3) * (8 * MP + 3 * MS)
+        return 37 * MP + 16 * MS + (dbl - 1) * (2 * MP + 5 * MS) + (add - 3) * (8 * MP + 3 * MS)
 
     def fft_products(inverse):
         tot = 0.0

@@ -364,16 +364,16 @@ struct DeviceGuard {  // make ctx->device current for the duration of a call
 constexpr double MP = 300.0, MS = 234.0, MR = 136.0, ADD_P = 12 * MP, MADD_P = 8 * MP + 2 * MS,
                  DBL_P = 6 * MP + 2 * MS;
 
-// A twiddle program (scalar_prog.cuh): 2P, 3P, 5P, 7P with the complete
-// projective formulas (1 doubling + 3 additions), the four points made affine
-// on the isomorphic curve with their phi images (27 M) and the result brought
-// back (3 M + 1 S), then Jacobian doublings (2 M + 5 S) and mixed additions
-// (8 M + 3 S) for the digits (program_cost counts the precompute's doubling
-// and three additions with them).
+// A twiddle program (scalar_prog.cuh): P to Jacobian (2 M + 1 S), 2P with P
+// on its Z (2 M + 5 S), 3P, 5P, 7P by co-Z additions (3 x (5 M + 2 S)), the
+// points brought onto one Z (11 M + 3 S) with their phi images (4 M), the
+// result brought back (3 M + 1 S): 37 M + 16 S; then Jacobian doublings
+// (2 M + 5 S) and mixed additions (8 M + 3 S) for the digits (program_cost
+// counts the precompute's doubling and three additions with them).
 double prog_products(int idx) {
     const HostConsts &hc = host_consts();
     if (hc.prog[idx][0] & 0x300u) return 0.0;
-    return DBL_P + 3 * ADD_P + 30.0 * MP + MS + (hc.prog_dbl[idx] - 1) * (2 * MP + 5 * MS) +
+    return 37.0 * MP + 16.0 * MS + (hc.prog_dbl[idx] - 1) * (2 * MP + 5 * MS) +
            (hc.prog_add[idx] - 3) * (8 * MP + 3 * MS);
 }
 

@@ -259,6 +259,66 @@ FK_HD void g1j_dbl(G1J &R, const G1J &P) {
     f_sub(R.y, t, C);     // Y3 = E (D - X3) - 8 C
 }
 
+// R = 2P and S = P moved onto the Z of R: S = (X (2Y)^2, Y (2Y)^3, 2 Y Z),
+// which dbl-2009-l computes anyway as (D, 8 C, Z3) ("DBLU" of the co-Z
+// literature); 2 M + 5 S.  R and S may alias P.
+FK_HD void g1j_dblu(G1J &R, G1J &S, const G1J &P) {
+    Fp A, B, C, D, t, y3;
+    fp_mul(t, P.y, P.z);  // Y Z
+    fp_sqr(B, P.y);       // B = Y^2
+    fp_sqr(A, P.x);       // A = X^2
+    fp_sqr(C, B);         // C = Y^4
+    f_add(D, P.x, B);
+    fp_sqr(D, D);
+    f_sub(D, D, A);
+    f_sub(D, D, C);
+    f_add(D, D, D);       // D = 4 X Y^2
+    f_add(t, t, t);       // Z3 = 2 Y Z
+    f_add(B, A, A);
+    f_add(A, B, A);       // E = 3 A
+    fp_sqr(B, A);         // F = E^2
+    f_sub(B, B, D);
+    f_sub(B, B, D);       // X3 = F - 2 D
+    f_add(C, C, C);
+    f_add(C, C, C);
+    f_add(C, C, C);       // 8 C
+    f_sub(y3, D, B);
+    fp_mul(y3, A, y3);
+    f_sub(y3, y3, C);     // Y3 = E (D - X3) - 8 C
+    R.x = B;
+    R.y = y3;
+    R.z = t;
+    S.x = D;
+    S.y = C;
+    S.z = t;
+}
+
+// Co-Z addition (Meloni, "ZADDU"): A = (X1, Y1, Z) and B = (X2, Y2, Z) share
+// Z, A != +-B.  R = A + B with Z3 = Z e, e = X2 - X1, and A is moved onto
+// that Z: A = (X1 e^2, Y1 e^3, Z e); e is returned.  5 M + 2 S.  R may alias
+// B (not A).
+FK_HD void g1j_zaddu(G1J &R, G1J &A, const G1J &B, Fp &e) {
+    Fp c, w1, w2, d, h, x3;
+    f_sub(e, B.x, A.x);    // e = X2 - X1
+    fp_sqr(c, e);          // e^2
+    fp_mul(w1, A.x, c);    // W1 = X1 e^2
+    fp_mul(w2, B.x, c);    // W2 = X2 e^2
+    f_sub(h, B.y, A.y);    // Y2 - Y1
+    fp_sqr(d, h);          // (Y2 - Y1)^2
+    f_sub(c, w2, w1);      // e^3
+    fp_mul(c, A.y, c);     // Y1 e^3
+    f_sub(x3, d, w1);
+    f_sub(x3, x3, w2);     // X3 = (Y2 - Y1)^2 - W1 - W2
+    f_sub(d, w1, x3);
+    fp_mul(d, h, d);
+    f_sub(R.y, d, c);      // Y3 = (Y2 - Y1) (W1 - X3) - Y1 e^3
+    fp_mul(A.z, A.z, e);   // Z3 = Z e
+    R.x = x3;
+    R.z = A.z;
+    A.x = w1;
+    A.y = c;
+}
+
 // R = P + (negQ ? -Q : Q) with Q = (x, y) affine, read through an accessor
 // (get(0) = x, get(1) = y); 8 M + 3 S ("madd-2007-bl" with Z3 = 2 Z1 H).
 // NOT complete: P = +-Q (H = 0) and P = infinity give wrong results.  The

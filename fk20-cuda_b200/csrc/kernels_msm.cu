@@ -12,7 +12,12 @@
 // (the complete projective one 11 M); its exceptional cases -- accumulator at
 // infinity, equal or opposite points -- are tested and handled, so every sum
 // is exact.  The result goes back to homogeneous projective coordinates.
-#if defined(FK_MSM_OUTLINE) && FK_MSM_OUTLINE
+// The Fp product and square out of line (one shared copy each): the mixed
+// addition's ten inlined products overflowed the instruction cache.
+#ifndef FK_MSM_OUTLINE
+#define FK_MSM_OUTLINE 1
+#endif
+#if FK_MSM_OUTLINE
 #define FK_FP_MUL_OUTLINE 1
 #endif
 #include <algorithm>
@@ -24,10 +29,12 @@
 #ifndef FK_MSM_MINB
 #define FK_MSM_MINB 1
 #endif
-// largest block size the launcher may use (64, 128 or 256 threads; the
-// launch bounds cap registers at 65536 / (FK_MSM_MAX_THREADS * FK_MSM_MINB))
+// largest block size the launcher may use; the launch bounds cap registers
+// at 65536 / (FK_MSM_MAX_THREADS * FK_MSM_MINB): 384 gives 168 registers, so
+// three 128-thread blocks (12 warps) fit an SM (64-, 128- and 256-thread
+// blocks launch as they are)
 #ifndef FK_MSM_MAX_THREADS
-#define FK_MSM_MAX_THREADS 256
+#define FK_MSM_MAX_THREADS 384
 #endif
 constexpr int MSM_MAX_THREADS = FK_MSM_MAX_THREADS;
 

@@ -68,20 +68,22 @@ struct SlotQ {
 // infinity), P read from point 0 of the slots, result in homogeneous
 // projective coordinates.
 //
-// 1. 2P, 3P = P + 2P, 5P, 7P with the complete projective formulas.
-// 2. The four points are made affine without an inversion, on the isomorphic
-//    curve E': y^2 = x^3 + b u^6 with u = Z_P Z_3P Z_5P Z_7P, which
-//    (x, y) -> (u^2 x, u^3 y) maps them to: x'_i = X_i u (u / Z_i),
-//    y'_i = Y_i u^2 (u / Z_i) (the products u / Z_i of the other three Z).
+// 1. P to Jacobian coordinates; 2P with P moved onto its Z (the doubling
+//    gives that for free), then 3P, 5P, 7P by co-Z additions of 2P (Meloni),
+//    each of which moves 2P onto the new Z; P, 3P and 5P are then brought
+//    onto the Z of 7P, u, by their steps' factors.  The four points share
+//    Z = u: their (x, y) are affine coordinates on the isomorphic curve
+//    E': y^2 = x^3 + b u^6, which (x, y) -> (u^2 x, u^3 y) maps E to, and
 //    phi commutes with the isomorphism, so phi of a table point is
-//    (beta x', y') there too.
-// 3. The digits run on E' with a Jacobian accumulator: doublings of 7 and
+//    (beta x', y') there too.  No exceptional case for points of order r
+//    (2P != +-P, 3P != +-2P, 5P != +-2P).
+// 2. The digits run on E' with a Jacobian accumulator: doublings of 7 and
 //    mixed additions of 11 Fp products (instead of 8 and 12 for the complete
 //    projective formulas), as neither formula uses b.  The mixed addition is
 //    not complete; for points of order r the accumulator never equals the
 //    added point or its negative, nor infinity (the program's partial sums,
 //    checked on the CPU for every program the library builds).
-// 4. Back to E: Jacobian (X, Y, Z u), i.e. homogeneous (X Z', Y, Z'^3) with
+// 3. Back to E: Jacobian (X, Y, Z u), i.e. homogeneous (X Z', Y, Z'^3) with
 //    Z' = Z u.  P = infinity (u = 0) makes every value above meaningless;
 //    the lane's flag then selects infinity.
 template <class ProgPtr>
@@ -97,57 +99,60 @@ FK_HD void g1_mul_prog(G1P &acc, const ProgSlots &slot, ProgPtr prog) {
     const int st = slot.stride;
     bool inf;
     {
-        // 2P parked in point 3; 3P = P + 2P, 5P = 3P + 2P, 7P = 5P + 2P
-        slot.pt(0).load(acc);
-        inf = f_is_zero(acc.z);
-        g1_dbl(acc, acc);
-        slot.pt(3).put(acc);
-        slot.pt(0).load(acc);
+        // P: homogeneous (X, Y, Z) -> Jacobian (X Z, Y Z^2, Z)
+        G1P p;
+        slot.pt(0).load(p);
+        inf = f_is_zero(p.z);
+        G1J a, b;
+        Fp t;
+        fp_sqr(t, p.z);
+        fp_mul(b.x, p.x, p.z);
+        fp_mul(b.y, p.y, t);
+        b.z = p.z;
+        // a = 2P, b = P on the Z of 2P; then b = 3P, 5P, 7P by co-Z additions
+        // of a, each of which moves a (2P) onto the new Z.  Point i keeps its
+        // (x, y); the factor e of its step waits in its beta x place.
+        g1j_dblu(a, b, b);
+        slot_put(slot.word(0), st, b.x);
+        slot_put(slot.word(12), st, b.y);
 #pragma unroll 1
         for (int i = 1; i < PROG_SLOTS; i++) {
-            g1_add_q(acc, acc, slot.pt(3), false);
-            slot.pt(i).put(acc);
+            g1j_zaddu(b, a, b, t);
+            slot_put(slot.word(36 * i), st, b.x);
+            slot_put(slot.word(36 * i + 12), st, b.y);
+            slot_put(slot.word(36 * i + 24), st, t);
         }
+        slot_put(slot.word(144), st, b.z);  // u: the Z of 7P
     }
     {
-        // u = Z0 Z1 Z2 Z3; lambda_i = u / Z_i written over Z_i
-        Fp z0, z1, z2, z3, a, b, t;
-        slot_get(z0, slot.word(24), st);
-        slot_get(z1, slot.word(36 + 24), st);
-        slot_get(z2, slot.word(72 + 24), st);
-        slot_get(z3, slot.word(108 + 24), st);
-        fp_mul(a, z0, z1);
-        fp_mul(b, z2, z3);
-        fp_mul(t, z1, b);
-        slot_put(slot.word(24), st, t);
-        fp_mul(t, z0, b);
-        slot_put(slot.word(36 + 24), st, t);
-        fp_mul(t, a, z3);
-        slot_put(slot.word(72 + 24), st, t);
-        fp_mul(t, a, z2);
-        slot_put(slot.word(108 + 24), st, t);
-        fp_mul(t, a, b);
-        slot_put(slot.word(144), st, t);
-    }
-    {
-        Fp u, beta, m, c;
-        slot_get(u, slot.word(144), st);
+        // onto the Z of 7P: 5P by e3, 3P by e2 e3, P by e1 e2 e3
+        // ((x, y) -> (f^2 x, f^3 y)); then beta x' of every point
+        Fp f, g, f2, c;
+        slot_get(f, slot.word(36 * 3 + 24), st);
+#pragma unroll 1
+        for (int i = PROG_SLOTS - 2; i >= 0; i--) {
+            if (i < PROG_SLOTS - 2) {
+                slot_get(g, slot.word(36 * (i + 1) + 24), st);
+                fp_mul(f, f, g);
+            }
+            uint32_t *q = slot.word(36 * i);
+            fp_sqr(f2, f);
+            slot_get(c, q, st);
+            fp_mul(c, c, f2);
+            slot_put(q, st, c);
+            fp_mul(f2, f2, f);
+            slot_get(c, q + 12 * st, st);
+            fp_mul(c, c, f2);
+            slot_put(q + 12 * st, st, c);
+        }
 #pragma unroll
-        for (int i = 0; i < 12; i++) beta.w[i] = beta_mont(i);
+        for (int i = 0; i < 12; i++) f.w[i] = beta_mont(i);
 #pragma unroll 1
         for (int i = 0; i < PROG_SLOTS; i++) {
-            uint32_t *p = slot.word(36 * i);
-            slot_get(m, p + 24 * st, st);
-            fp_mul(m, u, m);  // u lambda_i
-            slot_get(c, p, st);
-            fp_mul(c, c, m);  // x'_i
-            slot_put(p, st, c);
-            fp_mul(c, c, beta);
-            slot_put(p + 24 * st, st, c);  // beta x'_i
-            fp_mul(m, m, u);  // u^2 lambda_i
-            slot_get(c, p + 12 * st, st);
-            fp_mul(c, c, m);  // y'_i
-            slot_put(p + 12 * st, st, c);
+            uint32_t *q = slot.word(36 * i);
+            slot_get(c, q, st);
+            fp_mul(c, c, f);
+            slot_put(q + 24 * st, st, c);  // beta x'
         }
     }
     G1J j;
