@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--serve-fft-blocks", type=int, default=0,
                     help="persistent-FFT blocks per SM of each pack (0: adaptive to the backlog)")
+    ap.add_argument("--serve-max-queue", type=int, default=640,
+                    help="waiting requests beyond which the server refuses submits with FK20_EAGAIN (overload "
+                         "control; the client drops refused requests and counts them)")
     ap.add_argument("--serve-burst-rows", type=int, default=0,
                     help="pack size while more than 2 x max rows requests wait (0: 7/5 of max rows)")
     ap.add_argument("--serve-latency-rows", type=int, default=0,
@@ -375,6 +378,8 @@ def run_ours(args, ws, rank, dev):
         "peak_source": "measured live: fk20_bench_imad (8 independent IMAD chains/thread), IMAD/s / 2",
         "whole_step": {"achieved": all_prod / (all_ms * 1e-3) / 1e9, "frac": all_prod / (all_ms * 1e-3) / peak_products},
         "per_kind_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()},
+        # every kernel kind against the same peak: algorithmic products / its own launch time
+        "per_kind_frac": {k: (v[2] / (v[0] * 1e-3)) / peak_products for k, v in prof.items() if v[0] > 0},
         "products_per_launch": kprod / klaunch if klaunch else None,
     }
     if kind == "fft_fused" and klaunch:
@@ -554,7 +559,8 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
     weights = np.array([w for _, w in SERVE_MIX])
     mean_proofs = float((sizes // 8 * weights).sum())
     srv = E.Server(ctx, max_rows=args.serve_max_rows, slots=args.serve_slots, fft_blocks_per_sm=args.serve_fft_blocks,
-                   latency_rows=args.serve_latency_rows, burst_rows=args.serve_burst_rows)
+                   latency_rows=args.serve_latency_rows, burst_rows=args.serve_burst_rows,
+                   max_queue=args.serve_max_queue)
     loads = []
     rng = np.random.default_rng(42)
     check = []  # (n, pool index, output) kept for the bit-exactness check
@@ -587,6 +593,7 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
         due = start
         warm = warmup_s > 0
         lag = 0.0  # how far the client fell behind the arrival schedule
+        refused = 0
         for j in range(count):
             if warm and due - start >= warmup_s:
                 srv.reset_stats()  # steady state: later completions only
@@ -598,7 +605,14 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
             nj = int(lens[j])
             out = free[nj].pop() if free[nj] else np.zeros((nj // 8, 18), np.uint64)
             lag = max(lag, time.perf_counter() - due)
-            t = srv.submit(pool[nj][j % 24], out)
+            try:
+                t = srv.submit(pool[nj][j % 24], out)
+            except E.Fk20Error as err:
+                if err.code != E.FK20_EAGAIN:
+                    raise
+                refused += 1  # overload: the queue is full; the request is dropped
+                free[nj].append(out)
+                continue
             pending.put((t, nj, j, out))
         submit_s = time.perf_counter() - start
         pending.put(None)
@@ -615,6 +629,8 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
                       "mean_wait_ms": st["mean_wait_ms"], "mean_enqueue_ms": st["mean_enqueue_ms"],
                       "mean_run_ms": st["mean_run_ms"],
                       "errors": sum(1 for r in done_rc if r != 0),
+                      # admission: submits refused with FK20_EAGAIN (max_queue requests waiting)
+                      "admitted": count - refused, "refused": refused,
                       # the load generator itself: requests/s it achieved against the schedule's
                       "arrivals_per_s": {"offered": rate, "achieved": count / submit_s},
                       "client_max_lag_ms": lag * 1e3})
@@ -632,6 +648,7 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
                    "slots": args.serve_slots, "fft_blocks_per_sm": args.serve_fft_blocks or "adaptive",
                    "latency_rows": args.serve_latency_rows or args.serve_max_rows,
                    "burst_rows": args.serve_burst_rows or min(4096, args.serve_max_rows * 7 // 5),
+                   "max_queue": args.serve_max_queue,
                    "arrival_window_s": seconds, "warmup_s_excluded": warmup_s,
                    "table_bytes": ctx.device_bytes()},
         "plain_batch": {"rows": rows, "n": n, "proofs_per_s": plain_pps, "latency_ms": plain_ms},
