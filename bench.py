@@ -47,7 +47,9 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--rows", type=int, default=512)
     ap.add_argument("--n", type=int, default=4096)
-    ap.add_argument("--window", type=int, default=13)
+    ap.add_argument("--window", type=int, default=15,
+                    help="table window of the 4096-coefficient tables (117 GB at 15); the 1024- and "
+                         "2048-coefficient tables of the ragged and served loads use min(window, 13)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=0, help="rows per CPU sample (default: one per core)")
@@ -133,6 +135,19 @@ def max_over_ranks(x: float, ws: int) -> float:
     t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def load_other_lengths(ctx, args, n_main: int):
+    """Tables of the 1024- and 2048-coefficient lengths (the ragged and served
+    loads), at min(window, 13): with window 15 for 4096 (117 GB) all three
+    lengths at 15 would not fit the device."""
+    import fk20b200 as E
+    main_w = ctx.get(E.FK20_OPT_WINDOW)
+    ctx.set(E.FK20_OPT_WINDOW, min(main_w, 13))
+    for n2 in (1024, 2048, 4096):
+        if n2 != n_main:
+            ctx.load_setup(n2, gpu_setup(E, n2))
+    ctx.set(E.FK20_OPT_WINDOW, main_w)
 
 
 def rank_rows_seed(rank: int) -> int:
@@ -393,9 +408,16 @@ def run_ours(args, ws, rank, dev):
 
     # ---- e2e: reference entry point, host buffers, copies inside the timed region
     e2e = None
+    table_bytes = ctx.device_bytes()
     if not args.no_e2e:
         xext = E.empty((L, m, 18))
         E.call("fk20_setup2xext_fft", E._ptr(xext), E._ptr(setup), E._stream())
+        # the reference-signature entry point keeps its own tables in a
+        # process-wide default context: free this context's first (two sets
+        # at window 15 would not fit), and the default context's afterwards
+        torch.cuda.synchronize()
+        ctx.close()
+        ctx = None
         host_poly = torch.from_numpy(poly_h.view(np.int64)).pin_memory()
         host_out = torch.empty((rows, m, 18), dtype=torch.int64).pin_memory()
         dpoly = torch.empty_like(host_poly, device="cuda")
@@ -428,6 +450,8 @@ def run_ours(args, ws, rank, dev):
         dchk = host_out.cuda()
         E.call("g1p_eq_n", E._ptr(eq), E._ptr(dchk), E._ptr(h_fft), rows * m, E._stream())
         same = int(eq.sum()) == rows * m
+        torch.cuda.synchronize()
+        E.call("fk20_default_release", dev)
         e2e = {"value": ws * proofs * args.steps / (e_total * 1e-3), "unit": "proofs/s",
                "h2d_bytes_per_step": rows * n * 32, "d2h_bytes_per_step": rows * m * 144,
                "ms_per_step": e_total / args.steps, "path": "C-ABI fk20_poly2h_fft (fk20_poly2h_fft.cu:47)",
@@ -454,9 +478,10 @@ def run_ours(args, ws, rank, dev):
     ragged = served = None
     if ws == 1 and not args.no_records:
         del poly, h_fft
-        for n2 in (1024, 2048):
-            if n2 != n:
-                ctx.load_setup(n2, gpu_setup(E, n2))
+        if ctx is None:
+            ctx = E.Context(dev, args.window)
+            ctx.load_setup(n, setup)
+        load_other_lengths(ctx, args, n)
         torch.cuda.synchronize()
         with ClockSampler(dev) as rclk:
             ragged = ragged_on(ctx, rank, 5, 3)
@@ -471,11 +496,12 @@ def run_ours(args, ws, rank, dev):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded uniform Fr, seeded tau)",
         "config": workload_config(args, {"setup_s": round(setup_s, 2),
-                                         "table_bytes": ctx.device_bytes(), "autotune": tune}),
+                                         "table_bytes": table_bytes, "autotune": tune}),
         "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "ragged": ragged, "served": served, "impl": "ours",
     }
-    ctx.close()
+    if ctx is not None:
+        ctx.close()
     return line
 
 
@@ -505,8 +531,8 @@ def run_serve(args, ws, rank, dev):
     torch.cuda.set_device(dev)
     t0 = time.time()
     ctx = E.Context(dev, args.window)
-    for n, _ in SERVE_MIX:
-        ctx.load_setup(n, gpu_setup(E, n))
+    ctx.load_setup(4096, gpu_setup(E, 4096))
+    load_other_lengths(ctx, args, 4096)
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     # plain-batch capacity and latency: the full 512 x 4096 batch, device resident
@@ -644,7 +670,8 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
     return {
         "config": {"workload": "served load: Poisson arrivals of 1024/2048/4096-coefficient requests "
                                "(weights 0.2/0.3/0.5) at fractions of plain-batch capacity",
-                   "window_bits": args.window, "max_rows_per_pack": args.serve_max_rows,
+                   "window_bits": {"4096": args.window, "1024/2048": min(args.window, 13)},
+                   "max_rows_per_pack": args.serve_max_rows,
                    "slots": args.serve_slots, "fft_blocks_per_sm": args.serve_fft_blocks or "adaptive",
                    "latency_rows": args.serve_latency_rows or args.serve_max_rows,
                    "burst_rows": args.serve_burst_rows or min(4096, args.serve_max_rows * 7 // 5),
@@ -671,8 +698,8 @@ def run_ragged(args, ws, rank, dev):
 
     torch.cuda.set_device(dev)
     ctx = E.Context(dev, args.window)
-    for n in (1024, 2048, 4096):
-        ctx.load_setup(n, gpu_setup(E, n))
+    ctx.load_setup(4096, gpu_setup(E, 4096))
+    load_other_lengths(ctx, args, 4096)
     tune = None
     if args.autotune:
         tune = ctx.autotune(4096, rows=128, max_table_bytes=0)
@@ -685,7 +712,7 @@ def run_ragged(args, ws, rank, dev):
         "data": "synthetic (seeded uniform Fr, seeded tau)",
     }
     line.update(rec)
-    line["config"]["window_bits"] = args.window
+    line["config"]["window_bits"] = {"4096": args.window, "1024/2048": min(args.window, 13)}
     line["autotune"] = tune
     line["impl"] = "ours"
     ctx.close()

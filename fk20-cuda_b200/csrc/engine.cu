@@ -164,27 +164,36 @@ int log_m_for_n(unsigned n) {
 }
 
 constexpr unsigned MAX_ROWS = 1u << 20;
+// The FK20 MSM's tables cover the 128-bit GLV halves of the scalars (glv.cuh;
+// signed digits need one bit more); windows 8..15.
+constexpr int GLV_TABLE_BITS = 129;
+constexpr int MAX_WINDOW = 15;
 
+// A device buffer that only grows.  The buffer it outgrows may still be read
+// by work queued on any stream, and cudaFree would wait for the whole device
+// (stalling, for instance, a server's other packs): it is kept until
+// release() instead, when the owner is torn down.  Growth is geometric in
+// practice (a larger batch, a longer polynomial), so the kept buffers hold
+// less than the live one.
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    std::vector<void *> outgrown;
     int reserve(size_t need) {
         if (need <= bytes) return 0;
-        if (p) {
-            cudaDeviceSynchronize();  // the old buffer may still be in use by queued work
-            cudaFree(p);
-        }
-        p = nullptr;
-        bytes = 0;
-        if (cudaMalloc(&p, need) != cudaSuccess) {
+        void *q = nullptr;
+        if (cudaMalloc(&q, need) != cudaSuccess) {
             cudaGetLastError();
-            p = nullptr;
             return FK20_ENOMEM;
         }
+        if (p) outgrown.push_back(p);
+        p = q;
         bytes = need;
         return 0;
     }
     void release() {
+        for (void *q : outgrown) cudaFree(q);
+        outgrown.clear();
         if (p) cudaFree(p);
         p = nullptr;
         bytes = 0;
@@ -433,10 +442,11 @@ int output_launch(Profiler &pf, uint64_t *dst, const uint4 *D, const size_t *row
 }
 
 // Fixed-base tables of `nbases` bases (reference g1p_t on the device) at
-// window cb, every base first multiplied by program prog_scale (< 0: none).
+// window cb, every base first multiplied by program prog_scale (< 0: none),
+// for scalars of `bits` bits (W = ceil(bits / cb) windows).
 int build_base_tables(fk20_ctx *ctx, DevBuf &table, const uint64_t *bases, int nbases, int cb, int prog_scale,
-                      cudaStream_t st) {
-    const int W = (255 + cb - 1) / cb;
+                      int bits, cudaStream_t st) {
+    const int W = (bits + cb - 1) / cb;
     const int E = 1 << (cb - 1);
     const size_t entries = (size_t)nbases * W * E;
     table.release();
@@ -464,7 +474,7 @@ int build_tables(fk20_ctx *ctx, int log_m, const uint64_t *xext, cudaStream_t st
     Tables *T = tables_for(ctx, log_m);
     const int m = 1 << log_m;
     const int cb = ctx->window;
-    const int W = (255 + cb - 1) / cb;
+    const int W = (GLV_TABLE_BITS + cb - 1) / cb;
     T->ready = false;
     T->gen++;
     if (xext != (const uint64_t *)T->xext.p) {  // keep the bases for rebuilds at another window
@@ -473,7 +483,7 @@ int build_tables(fk20_ctx *ctx, int log_m, const uint64_t *xext, cudaStream_t st
         xext = (const uint64_t *)T->xext.p;
     }
     // the inverse FFT's 1/m folded into the bases (program 512 + log m = 2^-log m)
-    CKR(build_base_tables(ctx, T->table, xext, L_COLS * m, cb, 512 + log_m, st));
+    CKR(build_base_tables(ctx, T->table, xext, L_COLS * m, cb, 512 + log_m, GLV_TABLE_BITS, st));
     T->n = (unsigned)(m * L_COLS / 2);
     T->log_m = log_m;
     T->cb = cb;
@@ -501,7 +511,7 @@ int msm_launch(fk20_ctx *ctx, Tables *T, uint4 *D, const uint4 *S, int G, int ro
     a.nseg = 1;
     a.times_m = times_m;
     a.warps = (unsigned)G << T->log_m;
-    const double prod = (double)rows * L_COLS * (1 << T->log_m) * T->W * MADD_P +
+    const double prod = (double)rows * (1 << T->log_m) * (L_COLS * 2 * T->W * MADD_P + MP) +
                         (times_m ? (double)rows * (1 << T->log_m) * T->log_m * DBL_P : 0.0);
     ctx->prof.begin(FK20_K_MSM, prod, st);
     launch_msm(a, ctx->msm_threads, st);
@@ -590,7 +600,8 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
         a.seg[k] = MsmSeg{D + lay.d_off[k] / U, S + lay.s_off[k] / U, (const uint4 *)T->table.p, G, sg[k].log_m,
                           (int)sg[k].rows, T->cb, T->W, warps};
         warps += (unsigned)G * m;
-        prod += (double)sg[k].rows * L_COLS * m * T->W * MADD_P + (full ? 0.0 : (double)sg[k].rows * m * sg[k].log_m * DBL_P);
+        prod += (double)sg[k].rows * m * (L_COLS * 2 * T->W * MADD_P + MP) +
+                (full ? 0.0 : (double)sg[k].rows * m * sg[k].log_m * DBL_P);
     }
     a.nseg = nseg;
     a.times_m = full ? 0 : 1;
@@ -710,13 +721,24 @@ int default_ctx(fk20_ctx **out) {
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { cudaGetLastError(); return FK20_ENODEV; }
     std::lock_guard<std::mutex> lk(g_default_mu);
     if (!g_default[dev]) {
-        // FK20_WINDOW selects the default contexts' table window (8..13); unset = 10
+        // FK20_WINDOW selects the default contexts' table window (8..15); unset = 10
         int w = 0;
         if (const char *e = getenv("FK20_WINDOW")) w = atoi(e);
         CKR(fk20_ctx_create(&g_default[dev], dev, w));
     }
     *out = g_default[dev];
     return 0;
+}
+
+int release_default(int dev) {
+    if (dev < 0 || dev >= 64) return FK20_EINVAL;
+    fk20_ctx *c = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_default_mu);
+        c = g_default[dev];
+        g_default[dev] = nullptr;
+    }
+    return c ? fk20_ctx_destroy(c) : 0;
 }
 
 // tables of the default context keyed by the content of xext_fft (caller holds ctx->mu)
@@ -785,10 +807,12 @@ extern "C" {
 
 const char *fk20_version(void) { return FK20_VERSION; }
 
+int fk20_default_release(int device) { return release_default(device); }
+
 int fk20_ctx_create(fk20_ctx **out, int device, int window) {
     if (!out) return FK20_EINVAL;
     if (window == 0) window = 10;
-    if (window < 8 || window > 13) return FK20_EINVAL;
+    if (window < 8 || window > MAX_WINDOW) return FK20_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
         cudaGetLastError();
@@ -832,6 +856,10 @@ int fk20_ctx_set(fk20_ctx *ctx, int option, int value) {
         return 0;
     case FK20_OPT_TEST_UNPUBLISHED_TASK:
         ctx->unpublished = value < 0 ? 0xffffffffu : (unsigned)value;
+        return 0;
+    case FK20_OPT_WINDOW:
+        if (value < 8 || value > MAX_WINDOW) return FK20_EINVAL;
+        ctx->window = value;
         return 0;
     default: return FK20_EINVAL;
     }
@@ -995,6 +1023,7 @@ int fk20_ctx_get(fk20_ctx *ctx, int option, int *value) {
     switch (option) {
     case FK20_OPT_FUSED_FFT: *value = ctx->fused_fft; return 0;
     case FK20_OPT_MSM_THREADS: *value = ctx->msm_threads; return 0;
+    case FK20_OPT_WINDOW: *value = ctx->window; return 0;
     case FK20_OPT_FFT_BLOCKS_PER_SM: *value = ctx->fft_blocks_per_sm; return 0;
     case FK20_OPT_WAIT_LIMIT: *value = (int)ctx->wait_limit; return 0;
     case FK20_OPT_TEST_UNPUBLISHED_TASK: *value = ctx->unpublished == 0xffffffffu ? -1 : (int)ctx->unpublished; return 0;
@@ -1105,7 +1134,7 @@ int fk20_plan_destroy(fk20_plan *plan) {
 namespace {
 
 size_t table_bytes_for(int log_m, int w) {
-    const size_t W = (size_t)(255 + w - 1) / w;
+    const size_t W = (size_t)(GLV_TABLE_BITS + w - 1) / w;
     return (size_t)L_COLS * ((size_t)1 << log_m) * W * ((size_t)1 << (w - 1)) * 6 * sizeof(uint4);
 }
 
@@ -1198,7 +1227,7 @@ int autotune(fk20_ctx *ctx, int log_m, unsigned rows, size_t max_table_bytes, fk
             budget = fr + T->table.bytes > margin ? fr + T->table.bytes - margin : 0;
         }
         const int w0 = T->cb;
-        for (int w = 8; w <= 13 && !rc; w++) {
+        for (int w = 8; w <= MAX_WINDOW && !rc; w++) {
             if (w == w0 || table_bytes_for(log_m, w) > budget) continue;
             ctx->window = w;
             rc = build_tables(ctx, log_m, (const uint64_t *)T->xext.p, st);
@@ -1252,7 +1281,7 @@ int fk20_ctx_load_commit(fk20_ctx *ctx, unsigned n, const g1p_t *setup, int wind
     DeviceGuard dg(ctx->device);
     cudaStream_t st = S_(stream);
     ctx->commit.n = 0;
-    CKR(build_base_tables(ctx, ctx->commit.table, (const uint64_t *)setup, (int)n, window, -1, st));
+    CKR(build_base_tables(ctx, ctx->commit.table, (const uint64_t *)setup, (int)n, window, -1, 255, st));
     CK(cudaStreamSynchronize(st));
     ctx->commit.cb = window;
     ctx->commit.W = (255 + window - 1) / window;

@@ -4,6 +4,7 @@
 // points.  Fr data stays in standard form; twiddles are Montgomery constants,
 // so Montgomery products of data by twiddles return standard form.
 #include "consts.cuh"
+#include "glv.cuh"
 #include "launch.h"
 #include "layout.cuh"
 
@@ -54,6 +55,16 @@ __device__ void toeplitz_coef(Fr &v, const uint64_t *__restrict__ poly, int n, i
     }
 }
 
+// A scalar tile entry holds the GLV halves of the canonical scalar v:
+// uint4 0 = v mod lambda, uint4 1 (32 entries on) = v div lambda
+// (glv.cuh); the MSM's tables cover 128-bit scalars.
+__device__ __forceinline__ void store_scalar(uint4 *dst, const uint32_t v[8]) {
+    uint32_t s1[4], s2[4];
+    glv_split(s1, s2, v);
+    dst[0] = make_uint4(s1[0], s1[1], s1[2], s1[3]);
+    dst[32] = make_uint4(s2[0], s2[1], s2[2], s2[3]);
+}
+
 // grid (rows, 16), block m/2: toeplitz -> FFT -> scalar tiles S[g][c][i][q][lane]
 __global__ void __launch_bounds__(256) k_tc_fft(uint4 *__restrict__ S, const uint64_t *__restrict__ poly,
                                                const size_t *__restrict__ row_off, int n, int log_m) {
@@ -76,9 +87,7 @@ __global__ void __launch_bounds__(256) k_tc_fft(uint4 *__restrict__ S, const uin
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         const int c = tid + h * (m >> 1);
-        uint4 *dst = S + ((((size_t)g * m + c) * L_COLS + i) * SCAL_Q) * 32 + lane;
-        dst[0] = make_uint4(sm[c][0], sm[c][1], sm[c][2], sm[c][3]);
-        dst[32] = make_uint4(sm[c][4], sm[c][5], sm[c][6], sm[c][7]);
+        store_scalar(S + ((((size_t)g * m + c) * L_COLS + i) * SCAL_Q) * 32 + lane, sm[c]);
     }
 }
 
@@ -143,9 +152,7 @@ __global__ void k_ref_to_scalars(uint4 *__restrict__ S, const uint64_t *__restri
         Fr v;
         fr_from_ref(v, tcf + 4 * e);
         const int g = row >> 5, lane = row & 31;
-        uint4 *dst = S + ((((size_t)g * m + c) * L_COLS + i) * SCAL_Q) * 32 + lane;
-        dst[0] = make_uint4(v.w[0], v.w[1], v.w[2], v.w[3]);
-        dst[32] = make_uint4(v.w[4], v.w[5], v.w[6], v.w[7]);
+        store_scalar(S + ((((size_t)g * m + c) * L_COLS + i) * SCAL_Q) * 32 + lane, v.w);
     }
 }
 

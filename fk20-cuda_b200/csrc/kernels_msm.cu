@@ -172,21 +172,34 @@ __global__ void __launch_bounds__(MSM_MAX_THREADS, FK_MSM_MINB) k_msm(const __gr
     const int row = g * 32 + lane;
     const bool live = row < a.rows;
     const int E = 1 << (a.cb - 1);
+    // sum_i [s_i] X_i = phi(sum_i [s2_i] X_i) + sum_i [s1_i] X_i with
+    // s_i = s1_i + s2_i lambda (the scalar tile holds s1 at uint4 0 and s2 at
+    // uint4 1): the s2 halves first, then phi on the accumulator
+    // ((X, Y, ZZ, ZZZ) -> (beta X, Y, ZZ, ZZZ)), then the s1 halves.
     G1Z accz;
     g1z_set_inf(accz);
-    for (int i = 0; i < L_COLS; i++) {
-        uint32_t s[9];
-        const uint4 *src = a.S + ((((size_t)g * m + c) * L_COLS + i) * SCAL_Q) * 32 + lane;
-        const uint4 v0 = src[0], v1 = src[32];
-        s[0] = v0.x; s[1] = v0.y; s[2] = v0.z; s[3] = v0.w;
-        s[4] = v1.x; s[5] = v1.y; s[6] = v1.z; s[7] = v1.w;
-        s[8] = 0;
-        if (!live) {
+#pragma unroll 1
+    for (int half = 1; half >= 0; half--) {
+#pragma unroll 1
+        for (int i = 0; i < L_COLS; i++) {
+            uint32_t s[9];
+            const uint4 v = a.S[((((size_t)g * m + c) * L_COLS + i) * SCAL_Q + half) * 32 + lane];
+            s[0] = v.x; s[1] = v.y; s[2] = v.z; s[3] = v.w;
 #pragma unroll
-            for (int k = 0; k < 9; k++) s[k] = 0;
+            for (int k = 4; k < 9; k++) s[k] = 0;
+            if (!live) {
+#pragma unroll
+                for (int k = 0; k < 4; k++) s[k] = 0;
+            }
+            const uint4 *tb = a.table + ((size_t)(i * m + c) * a.W) * E * 6;
+            msm_add_scalar(accz, s, tb, a.W, a.cb);
         }
-        const uint4 *tb = a.table + ((size_t)(i * m + c) * a.W) * E * 6;
-        msm_add_scalar(accz, s, tb, a.W, a.cb);
+        if (half) {
+            Fp beta;
+#pragma unroll
+            for (int k = 0; k < 12; k++) beta.w[k] = beta_mont(k);
+            fp_mul(accz.x, accz.x, beta);
+        }
     }
     G1P acc;
     g1z_to_proj(acc, accz);

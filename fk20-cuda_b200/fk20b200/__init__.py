@@ -42,7 +42,7 @@ ABI_SYMBOLS = (
     "fk20_server_wait", "fk20_server_get_stats", "fk20_server_reset_stats", "fk20_server_destroy",
     "fk20_g1p_compress_n", "fk20_h_fft2proofs", "fk20_ctx_poly2proofs", "fk20_ctx_batch_proofs",
     "fk20_ctx_load_commit", "fk20_ctx_commit", "fk20_pairing_check_n", "fk20_pairing_n", "g2p_op_n",
-    "fk20_ctx_check_proof_multi",
+    "fk20_ctx_check_proof_multi", "fk20_default_release",
 )
 
 # kernel kinds of the per-launch profiler (FK20_K_* in the header)
@@ -55,6 +55,7 @@ FK20_OPT_MSM_THREADS = 2
 FK20_OPT_FFT_BLOCKS_PER_SM = 3
 FK20_OPT_WAIT_LIMIT = 4
 FK20_OPT_TEST_UNPUBLISHED_TASK = 5
+FK20_OPT_WINDOW = 6
 
 
 class TuneResult(ctypes.Structure):
@@ -165,6 +166,7 @@ def lib() -> ctypes.CDLL:
             "fk20_ctx_check_proof_multi": ([vp, vp, vp, vp, vp, vp, u, vp, u, vp], i),
             "fk20_pairing_n": ([vp, vp, vp, sz, vp], i),
             "g2p_op_n": ([i, vp, vp, vp, sz, vp], i),
+            "fk20_default_release": ([i], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

@@ -58,11 +58,13 @@ typedef struct { fp_t x, y, z; } g1p_t;
  */
 typedef struct fk20_ctx fk20_ctx;
 
-/* window: signed-digit width of the fixed-base tables (8..13; 0 = default 10).
- * Table bytes per polynomial length n: 16*m bases * ceil(255/w) windows *
- * 2^(w-1) entries * 96 B (10.5 GB for n = 4096, w = 10).  The default
- * context behind the reference-signature entry points takes its window from
- * the environment variable FK20_WINDOW (read once per device), else 10. */
+/* window: signed-digit width of the fixed-base tables (8..15; 0 = default 10).
+ * The MSM splits each scalar s = s1 + s2 lambda with the GLV endomorphism
+ * (s1, s2 < 2^128), so the tables cover 129-bit digits: bytes per polynomial
+ * length n: 16*m bases * ceil(129/w) windows * 2^(w-1) entries * 96 B
+ * (5.2 GB for n = 4096, w = 10; 116 GB at w = 15).  The default context
+ * behind the reference-signature entry points takes its window from the
+ * environment variable FK20_WINDOW (read once per device), else 10. */
 int fk20_ctx_create(fk20_ctx **ctx, int device, int window);
 int fk20_ctx_destroy(fk20_ctx *ctx);
 
@@ -114,7 +116,7 @@ int fk20_plan_launch(fk20_plan *plan, void *stream);
 int fk20_plan_destroy(fk20_plan *plan);
 
 /* Autotuner (no reference counterpart): times the pipeline for length n on
- * `rows` seeded sample rows under each candidate -- table window 8..13 whose
+ * `rows` seeded sample rows under each candidate -- table window 8..15 whose
  * tables fit in max_table_bytes (0 = what the free device memory allows),
  * MSM block size 64/128/256, persistent FFT grid 1..max blocks per SM, fused
  * or staged FFT -- one parameter at a time, keeps the fastest in the context
@@ -147,6 +149,13 @@ int fk20_ctx_autotune(fk20_ctx *ctx, unsigned n, unsigned rows, size_t max_table
  * the call's results are invalid (fk20_ctx_status returns FK20_ETIMEOUT and
  * clears the condition).  -1 (default) = off. */
 #define FK20_OPT_TEST_UNPUBLISHED_TASK 5
+/* FK20_OPT_WINDOW: table window (8..15) of the tables that later
+ * fk20_ctx_load_setup / fk20_ctx_load_xext_fft calls build (tables already
+ * built keep theirs), so each polynomial length can have its own: tables of
+ * length n hold 2n (ceil(129 / w)) 2^(w-1) entries of 96 bytes -- at n = 4096,
+ * 32 GB at w = 13 and 116 GB at w = 15 (9 instead of 10 windows per GLV
+ * half). */
+#define FK20_OPT_WINDOW 6
 int fk20_ctx_set(fk20_ctx *ctx, int option, int value);
 int fk20_ctx_get(fk20_ctx *ctx, int option, int *value);
 
@@ -319,6 +328,12 @@ int fk20_server_destroy(fk20_server *srv);
 
 /* fk20_poly2h_fft.cu:47 -- polynomial[rows][4096] + xext_fft[16][512] -> h_fft[rows][512] */
 int fk20_poly2h_fft(g1p_t *h_fft, const fr_t *polynomial, const g1p_t *xext_fft, unsigned rows);
+
+/* No counterpart in the reference (whose tables live in file-scope managed
+ * memory for the life of the process): frees the default context of `device`
+ * and its tables (117 GB at window 15); the next reference-signature call on
+ * that device builds them again.  No call may be in flight on it. */
+int fk20_default_release(int device);
 
 /* fk20_poly2toeplitz_coefficients.cu:25 -- polynomial[rows][4096] -> tc[rows][16][512] */
 int fk20_poly2toeplitz_coefficients(fr_t *toeplitz_coefficients, const fr_t *polynomial, unsigned rows,

@@ -5,6 +5,7 @@
 #include <cstring>
 #include "field.cuh"
 #include "g1.cuh"
+#include "glv.cuh"
 
 using namespace fk;
 
@@ -122,5 +123,23 @@ long emul_fused_schedule(int nseg, const int *G, const int *log_m, int *out, lon
         o[0] = f.seg; o[1] = f.S; o[2] = f.g; o[3] = f.i0; o[4] = f.i1; o[5] = f.tix; o[6] = f.kind;
     }
     return (long)total;
+}
+}
+
+extern "C" {
+// GLV split of count scalars (4 x u64 each, s < 2^255): out[2 i] = s mod lambda,
+// out[2 i + 1] = s div lambda (2 x u64 each, the upper two words zero)
+int emul_glv_split(uint64_t *out, const uint64_t *s, long count) {
+    for (long i = 0; i < count; i++) {
+        uint32_t w[8], a[4], b[4];
+        for (int k = 0; k < 4; k++) { w[2 * k] = (uint32_t)s[4 * i + k]; w[2 * k + 1] = (uint32_t)(s[4 * i + k] >> 32); }
+        glv_split(a, b, w);
+        for (int k = 0; k < 2; k++) {
+            out[8 * i + k] = (uint64_t)a[2 * k] | ((uint64_t)a[2 * k + 1] << 32);
+            out[8 * i + 4 + k] = (uint64_t)b[2 * k] | ((uint64_t)b[2 * k + 1] << 32);
+        }
+        out[8 * i + 2] = out[8 * i + 3] = out[8 * i + 6] = out[8 * i + 7] = 0;
+    }
+    return 0;
 }
 }

@@ -353,7 +353,8 @@ def test_autotune_keeps_results(engine):
     before = engine.empty((rows, m, 18))
     c.poly2h_fft(before, poly, rows, n)
     res = c.autotune(n, rows=64, max_table_bytes=3 << 30)
-    assert 8 <= res["window"] <= 10 and res["msm_threads"] in (64, 128, 256)
+    # n = 1024: window 11 takes 2.4 GB, 12 takes 4.4 GB (ceil(129 / w) windows per GLV half)
+    assert 8 <= res["window"] <= 11 and res["msm_threads"] in (64, 128, 256)
     assert res["ms"] <= res["ms_default"] * 1.05
     assert c.get(engine.FK20_OPT_MSM_THREADS) == res["msm_threads"]
     after = engine.empty((rows, m, 18))

@@ -1,12 +1,14 @@
 """The MSM's exceptional mixed additions on the GPU (kernels_msm.cu g1z_madd):
 the XYZZ accumulator equal to the added table entry (the doubling branch) and
 equal to its negation (the infinity branch), reached by positive and by
-negative signed digits, and the addition that follows an accumulator at
-infinity.  Random FK20 inputs never reach these branches; here the bases
-xext_fft[i][c] are all the generator G except base 2, which is -G, and the
-scalars are crafted per row, so the sums are known multiples of G.  The
-reference's fk20_msm (fk20_msm.cu:23-66) uses complete formulas and has no
-such branches: its result is the plain sum, which is what the oracle gives."""
+negative signed digits, in both GLV passes (the s2 = s div lambda halves,
+then phi, then the s1 = s mod lambda halves), and the addition that follows
+an accumulator at infinity.  Random FK20 inputs never reach these branches;
+here the bases xext_fft[i][c] are all the generator G except base 2, which
+is -G, and the scalars are crafted per row, so the sums are known multiples
+of G.  The reference's fk20_msm (fk20_msm.cu:23-66) uses complete formulas
+and has no such branches: its result is the plain sum, which is what the
+oracle gives."""
 import numpy as np
 import pytest
 
@@ -14,7 +16,8 @@ import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-CB = 8  # table window of the context below: digits in [-128, 128], 32 windows
+CB = 8  # table window of the context below: digits in [-128, 128], 17 windows per GLV half
+LAMBDA = 0xAC45A4010001A40200000000FFFFFFFF  # phi = [lambda] on G1
 
 
 def _scalar_rows(rows):
@@ -29,13 +32,17 @@ def _scalar_rows(rows):
     s[2, 0], s[2, 3] = 4, (1 << CB) - 4
     # 3: 4G, then 252 on -G: digit -4 gives +4G == accumulator -> doubling, then -256G
     s[3, 0], s[3, 2] = 4, (1 << CB) - 4
-    # 4: the doubling branch on a top-window entry: 2^248 G (window 31, digit 1) twice
-    s[4, 0], s[4, 1] = 1 << 248, 1 << 248
+    # 4: the doubling branch on a top-window entry: 2^120 G (window 15, digit 1) twice
+    s[4, 0], s[4, 1] = 1 << 120, 1 << 120
     # 5: all zero -> infinity
-    rnd = O.seeded_fr(515, (rows - 6) * 16)
-    for k in range(6, rows):
+    # 6: the s2 pass: 2 lambda = 0 + 2 lambda twice -> doubling there, then phi
+    s[6, 0], s[6, 1] = 2 * LAMBDA, 2 * LAMBDA
+    # 7: the s2 pass: 2 lambda on G, then on -G -> infinity there
+    s[7, 0], s[7, 2] = 2 * LAMBDA, 2 * LAMBDA
+    rnd = O.seeded_fr(515, (rows - 8) * 16)
+    for k in range(8, rows):
         for i in range(16):
-            s[k, i] = O.limbs_to_int(rnd[(k - 6) * 16 + i])
+            s[k, i] = O.limbs_to_int(rnd[(k - 8) * 16 + i])
     return s
 
 
@@ -63,7 +70,7 @@ def test_msm_exceptional_branches(engine):
         c.close()
     sign = [-1 if i == 2 else 1 for i in range(16)]
     ks = [sum(sign[i] * int(sc[r, i]) for i in range(16)) % O.R for r in range(rows)]
-    assert ks[:6] == [4, 5, 256, (4 - 252) % O.R, (1 << 249) % O.R, 0]
+    assert ks[:8] == [4, 5, 256, (4 - 252) % O.R, 1 << 121, 0, 4 * LAMBDA % O.R, 0]
     exp = O.g1_normalize(O.g1_op("mul", np.repeat(g.reshape(1, 18), rows, 0), O.ints_to_array(ks, 4)))
     for r in range(rows):
         assert np.array_equal(got[r], np.repeat(exp[r:r + 1], m, 0)), r

@@ -218,3 +218,21 @@ def test_programs_avoid_the_mixed_additions_exceptional_cases(emul):
             assert a != 0 and a != q and a != (r - q) % r, (hex(k), hex(a), hex(q))
         checked += len(adds)
     assert checked > 20000
+
+
+def test_glv_split_of_msm_scalars(emul):
+    """The MSM's scalar split (csrc/glv.cuh): s = s1 + s2 lambda with
+    s1 = s mod lambda and s2 = s div lambda, both below 2^128, for random
+    scalars below r and for the edges of the Barrett estimate."""
+    r = O.R
+    rng = np.random.default_rng(12)
+    xs = [int.from_bytes(rng.bytes(32), "little") % r for _ in range(4000)]
+    xs += [0, 1, LAMBDA - 1, LAMBDA, LAMBDA + 1, 2 * LAMBDA - 1, 2 * LAMBDA, r - 1, r - 2, r - LAMBDA,
+           LAMBDA * LAMBDA, LAMBDA * LAMBDA - 1, (1 << 255) - 1, (1 << 254), (1 << 128) - 1, 1 << 128]
+    s = O.ints_to_array(xs, 4)
+    out = np.zeros((len(xs), 8), np.uint64)
+    emul.emul_glv_split(P(out), P(s), len(xs))
+    for j, x in enumerate(xs):
+        s1, s2 = O.limbs_to_int(out[j, :4]), O.limbs_to_int(out[j, 4:])
+        assert (s1, s2) == (x % LAMBDA, x // LAMBDA), hex(x)
+        assert s1 < 1 << 128 and s2 < 1 << 128
