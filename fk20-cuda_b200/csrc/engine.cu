@@ -14,6 +14,7 @@
 // There is no CPU compute path: without a usable sm_100 device every entry
 // point returns FK20_ENODEV or the CUDA error.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -31,6 +32,7 @@
 #include <vector>
 
 #include "../../include/fk20_b200.h"
+#include "check.cuh"
 #include "consts.cuh"
 #include "launch.h"
 #include "layout.cuh"
@@ -169,6 +171,10 @@ constexpr unsigned MAX_ROWS = 1u << 20;
 constexpr int GLV_TABLE_BITS = 129;
 constexpr int MAX_WINDOW = 15;
 
+// the persistent FFT's error word: 1000 + stage when a bounded wait gave up,
+// 2000 when a check of the checked build stopped the launch
+int launch_error(int e) { return e >= 2000 ? FK20_ECHECK : FK20_ETIMEOUT; }
+
 // A device buffer that only grows.  The buffer it outgrows may still be read
 // by work queued on any stream, and cudaFree would wait for the whole device
 // (stalling, for instance, a server's other packs): it is kept until
@@ -271,8 +277,24 @@ struct Workspace {
 // pipeline kernel, with the algorithmic work of that launch (in 32x32->64-bit
 // limb products: Fp product M_p = 300, Fr product M_r = 136, RCB addition
 // 12 M_p, XYZZ mixed addition 10 M_p, doubling 8 M_p).
+// NVTX ranges per pipeline stage (toeplitz + Fr FFTs, MSM, G1 FFT stages,
+// output), named "fk20 <stage>", for nsys / ncu timelines: on when the
+// environment variable FK20_NVTX is set to a nonzero value (read once per
+// process).  Ranges are started and ended by id, so an error return between
+// a stage's launch and its end leaves no nesting unbalanced.
+bool nvtx_on() {
+    static const bool on = [] {
+        const char *e = getenv("FK20_NVTX");
+        return e && atoi(e) != 0;
+    }();
+    return on;
+}
+const char *const NVTX_STAGE[FK20_NKINDS] = {"fk20 tc_fft", "fk20 msm",    "fk20 stage_inv", "fk20 stage_fwd",
+                                             "fk20 middle", "fk20 output", "fk20 fft_fused"};
+
 struct Profiler {
     bool on = false;
+    nvtxRangeId_t nvtx = 0;
     struct Rec {
         int kind;
         double products;
@@ -293,12 +315,17 @@ struct Profiler {
         return e;
     }
     void begin(int kind, double prod, cudaStream_t st) {
+        if (nvtx_on()) nvtx = nvtxRangeStartA(NVTX_STAGE[kind]);
         if (!on) return;
         Rec r{kind, prod, get(), get()};
         cudaEventRecord(r.a, st);
         pending.push_back(r);
     }
     void end(cudaStream_t st) {
+        if (nvtx) {
+            nvtxRangeEnd(nvtx);
+            nvtx = 0;
+        }
         if (!on || pending.empty()) return;
         cudaEventRecord(pending.back().b, st);
     }
@@ -331,6 +358,7 @@ struct fk20_ctx {
     int sms = 148;
     int fused_fft = 1;          // run the G1 FFT stages as one persistent launch
     int msm_threads = 128;      // MSM block size (64, 128, 256)
+    int test_check = 0;         // checked build: MSM launches record a planted failure (tests)
     int fft_blocks_per_sm = 0;  // persistent FFT grid: blocks per SM (0 = as many as fit)
     int fused_occupancy = 1;    // blocks of the persistent FFT kernel that fit on one SM
     unsigned wait_limit = FUSED_SPIN_LIMIT;  // polls before a persistent wait gives up
@@ -510,6 +538,7 @@ int msm_launch(fk20_ctx *ctx, Tables *T, uint4 *D, const uint4 *S, int G, int ro
     a.seg[0] = MsmSeg{D, S, (const uint4 *)T->table.p, G, T->log_m, rows, T->cb, T->W, 0};
     a.nseg = 1;
     a.times_m = times_m;
+    a.test_check = ctx->test_check;
     a.warps = (unsigned)G << T->log_m;
     const double prod = (double)rows * (1 << T->log_m) * (L_COLS * 2 * T->W * MADD_P + MP) +
                         (times_m ? (double)rows * (1 << T->log_m) * T->log_m * DBL_P : 0.0);
@@ -580,7 +609,7 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
     SegLayout lay;
     CKR(segment_layout(ctx, sg, nseg, lay));
     CKR(reserve_segments(ctx, ws, sg, nseg, full));
-    if (*ws.err_host) return FK20_ETIMEOUT;  // a previous persistent launch gave up: its results are invalid
+    if (*ws.err_host) return launch_error(*ws.err_host);  // a previous persistent launch stopped: results invalid
     uint4 *S = (uint4 *)ws.S.p, *D = (uint4 *)ws.D.p;
     const size_t U = sizeof(uint4);
     for (int k = 0; k < nseg; k++) {
@@ -605,6 +634,7 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
     }
     a.nseg = nseg;
     a.times_m = full ? 0 : 1;
+    a.test_check = ctx->test_check;
     a.warps = warps;
     ctx->prof.begin(FK20_K_MSM, prod, st);
     launch_msm(a, ctx->msm_threads, st);
@@ -809,6 +839,14 @@ const char *fk20_version(void) { return FK20_VERSION; }
 
 int fk20_default_release(int device) { return release_default(device); }
 
+int fk20_check_status(int *compiled) {
+    if (compiled) *compiled = FK_CHECKED;
+    if (cudaDeviceSynchronize() != cudaSuccess) return (int)cudaGetLastError();
+    int v = check_take_msm();
+    const int f = check_take_fft();
+    return v ? v : f;
+}
+
 int fk20_ctx_create(fk20_ctx **out, int device, int window) {
     if (!out) return FK20_EINVAL;
     if (window == 0) window = 10;
@@ -861,6 +899,7 @@ int fk20_ctx_set(fk20_ctx *ctx, int option, int value) {
         if (value < 8 || value > MAX_WINDOW) return FK20_EINVAL;
         ctx->window = value;
         return 0;
+    case FK20_OPT_TEST_CHECK: ctx->test_check = value != 0; return 0;
     default: return FK20_EINVAL;
     }
 }
@@ -871,8 +910,9 @@ int fk20_ctx_status(fk20_ctx *ctx) {
     DeviceGuard dg(ctx->device);
     CK(cudaDeviceSynchronize());
     if (ctx->ws.err_host && *ctx->ws.err_host) {
+        const int rc = launch_error(*ctx->ws.err_host);
         *ctx->ws.err_host = 0;
-        return FK20_ETIMEOUT;
+        return rc;
     }
     return 0;
 }
@@ -1112,7 +1152,7 @@ int fk20_plan_launch(fk20_plan *plan, void *stream) {
     DeviceGuard dg(ctx->device);
     for (int k = 0; k < 3; k++)
         if (plan->gen[k] != ctx->tab[k].gen) return FK20_ENOSETUP;
-    if (*plan->ws.err_host) return FK20_ETIMEOUT;
+    if (*plan->ws.err_host) return launch_error(*plan->ws.err_host);
     CK(cudaGraphLaunch(plan->exec, S_(stream)));
     return 0;
 }
@@ -1156,8 +1196,9 @@ struct Tuner {
         CK(cudaEventRecord(e1, st));
         CK(cudaEventSynchronize(e1));
         if (*ctx->ws.err_host) {
+            const int rc = launch_error(*ctx->ws.err_host);
             *ctx->ws.err_host = 0;
-            return FK20_ETIMEOUT;
+            return rc;
         }
         CK(cudaEventElapsedTime(ms, e0, e1));
         *ms /= reps;
@@ -1763,8 +1804,8 @@ void server_main(fk20_server *s) {
                     cudaGetLastError();
                     status = (int)q;
                 } else if (*sl.ws.err_host) {
+                    status = launch_error(*sl.ws.err_host);
                     *sl.ws.err_host = 0;  // the next pack of this slot starts clean
-                    status = FK20_ETIMEOUT;
                 }
             }
             std::vector<Req> done;

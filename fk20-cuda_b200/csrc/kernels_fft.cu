@@ -15,6 +15,8 @@
 #if FK_FFT_OUTLINE
 #define FK_FP_MUL_OUTLINE 1
 #endif
+#include "../../include/fk20_b200.h"
+#include "check.cuh"
 #include "consts.cuh"
 #include "launch.h"
 #include "layout.cuh"
@@ -24,6 +26,8 @@
 namespace fk {
 
 cudaError_t upload_consts_fft() { return upload_module_consts(); }
+
+FK_CHECK_WORD(fft)
 
 // minimum resident blocks per SM requested from ptxas for the stage kernels
 // (caps registers at 65536 / (FFT_THREADS * FK_FFT_MINB))
@@ -164,6 +168,15 @@ __global__ void __launch_bounds__(FFT_THREADS, FK_FFT_MINB) k_g1_fused(const __g
         if (*(volatile int *)P.err) return;
         FusedTask t;
         fused_task_decode(t, P.blk, task);
+        // checked build: the decoded task lies in its segment and names a
+        // program; otherwise stop the launch (no access, no publication)
+        if (!FK_CHECK(g_check_fft, t.seg >= 0 && t.seg < P.blk.nseg && t.g >= 0 && t.g < P.blk.G[t.seg] &&
+                                       t.i0 >= 0 && t.i1 < (1 << P.blk.log_m[t.seg]) && t.i0 < t.i1,
+                      FK20_CHECK_FFT_TASK) ||
+            !FK_CHECK(g_check_fft, t.tix >= 0 && t.tix < NPROG, FK20_CHECK_FFT_PROGRAM)) {
+            if (lane == 0) atomicCAS(P.err, 0, 2000);
+            return;
+        }
         const FusedSeg &a = P.seg[t.seg];
         const int m = 1 << P.blk.log_m[t.seg];
         const int S = t.S, g = t.g, i0 = t.i0, i1 = t.i1, tix = t.tix, kind = t.kind;

@@ -22,6 +22,8 @@
 #endif
 #include <algorithm>
 
+#include "../../include/fk20_b200.h"
+#include "check.cuh"
 #include "consts.cuh"
 #include "launch.h"
 #include "layout.cuh"
@@ -41,6 +43,8 @@ constexpr int MSM_MAX_THREADS = FK_MSM_MAX_THREADS;
 namespace fk {
 
 cudaError_t upload_consts_msm() { return upload_module_consts(); }
+
+FK_CHECK_WORD(msm)
 
 // XYZZ point: x = X / ZZ, y = Y / ZZZ (ZZ^3 = ZZZ^2); ZZ = 0 is infinity
 struct G1Z {
@@ -124,7 +128,9 @@ FK_D void g1z_to_proj(G1P &r, const G1Z &a) {
 // window w and e < 2^(cb-1): the 255-bit scalar s (9 words, s[8] = 0) is
 // recoded into W signed digits in [-2^(cb-1), 2^(cb-1)] on the fly and every
 // nonzero digit costs one mixed addition of a gathered 96-byte entry.
-FK_D void msm_add_scalar(G1Z &acc, const uint32_t s[9], const uint4 *__restrict__ tb, int W, int cb) {
+// Returns the recoding's final carry: nonzero when s needs more than W
+// windows (the tables do not cover it).
+FK_D int msm_add_scalar(G1Z &acc, const uint32_t s[9], const uint4 *__restrict__ tb, int W, int cb) {
     const int E = 1 << (cb - 1);
     const uint32_t mask = (1u << cb) - 1u;
     int carry = 0;
@@ -154,6 +160,7 @@ FK_D void msm_add_scalar(G1Z &acc, const uint32_t s[9], const uint4 *__restrict_
             }
         }
     }
+    return carry;
 }
 
 // One warp per (segment, column c, group g of 32 rows); lanes are rows.
@@ -169,6 +176,8 @@ __global__ void __launch_bounds__(MSM_MAX_THREADS, FK_MSM_MINB) k_msm(const __gr
     const int lane = threadIdx.x & 31;
     const unsigned wl = warp - a.warp_start;
     const int g = (int)(wl % (unsigned)a.G), c = (int)(wl / (unsigned)a.G);
+    if (!FK_CHECK(g_check_msm, k < args.nseg && c < m, FK20_CHECK_MSM_TILE)) return;
+    if (args.test_check && warp == 0 && lane == 0) (void)FK_CHECK(g_check_msm, false, FK20_CHECK_MSM_PLANTED);
     const int row = g * 32 + lane;
     const bool live = row < a.rows;
     const int E = 1 << (a.cb - 1);
@@ -192,7 +201,8 @@ __global__ void __launch_bounds__(MSM_MAX_THREADS, FK_MSM_MINB) k_msm(const __gr
                 for (int k = 0; k < 4; k++) s[k] = 0;
             }
             const uint4 *tb = a.table + ((size_t)(i * m + c) * a.W) * E * 6;
-            msm_add_scalar(accz, s, tb, a.W, a.cb);
+            const int carry = msm_add_scalar(accz, s, tb, a.W, a.cb);
+            (void)FK_CHECK(g_check_msm, carry == 0, FK20_CHECK_MSM_CARRY);
         }
         if (half) {
             Fp beta;
@@ -239,7 +249,7 @@ __global__ void __launch_bounds__(128) k_commit_partial(uint4 *__restrict__ part
 #pragma unroll
             for (int k = 0; k < 8; k++) s[k] = f.w[k];
         }
-        msm_add_scalar(accz, s, table + (size_t)i * W * E * 6, W, cb);
+        (void)msm_add_scalar(accz, s, table + (size_t)i * W * E * 6, W, cb);
     }
     G1P acc;
     g1z_to_proj(acc, accz);

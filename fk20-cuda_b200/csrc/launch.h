@@ -25,6 +25,7 @@ struct MsmSeg {
 struct MsmArgs {
     MsmSeg seg[MAX_SEGS];
     int nseg, times_m;
+    int test_check;  // checked build: record FK20_CHECK_MSM_PLANTED (tests of the checks)
     unsigned warps;  // total warps = sum of G * m
 };
 
@@ -65,6 +66,10 @@ void launch_ref_to_scalars(uint4 *S, const uint64_t *tcf, int rows, int log_m, c
 
 // kernels_msm.cu
 void launch_msm(const MsmArgs &a, int threads, cudaStream_t st);  // threads: 64, 128 or 256
+// checked build (check.cuh): take and clear the first failing check site of the
+// MSM / persistent-FFT translation units (0: none)
+int check_take_msm();
+int check_take_fft();
 // KZG commitments: polynomial lengths are multiples of COMMIT_CHUNK; pass 1
 // has commit_parts(rows, n) warps per 32 rows, and part holds as many tiles
 constexpr int COMMIT_CHUNK = 32;

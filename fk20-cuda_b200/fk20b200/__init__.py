@@ -42,7 +42,7 @@ ABI_SYMBOLS = (
     "fk20_server_wait", "fk20_server_get_stats", "fk20_server_reset_stats", "fk20_server_destroy",
     "fk20_g1p_compress_n", "fk20_h_fft2proofs", "fk20_ctx_poly2proofs", "fk20_ctx_batch_proofs",
     "fk20_ctx_load_commit", "fk20_ctx_commit", "fk20_pairing_check_n", "fk20_pairing_n", "g2p_op_n",
-    "fk20_ctx_check_proof_multi", "fk20_default_release",
+    "fk20_ctx_check_proof_multi", "fk20_default_release", "fk20_check_status",
 )
 
 # kernel kinds of the per-launch profiler (FK20_K_* in the header)
@@ -50,12 +50,14 @@ KINDS = ("tc_fft", "msm", "stage_inv", "stage_fwd", "middle", "output", "fft_fus
 FK20_ETIMEOUT = 1005
 FK20_ETOOBIG = 1006
 FK20_EAGAIN = 1007
+FK20_ECHECK = 1008
 FK20_OPT_FUSED_FFT = 1
 FK20_OPT_MSM_THREADS = 2
 FK20_OPT_FFT_BLOCKS_PER_SM = 3
 FK20_OPT_WAIT_LIMIT = 4
 FK20_OPT_TEST_UNPUBLISHED_TASK = 5
 FK20_OPT_WINDOW = 6
+FK20_OPT_TEST_CHECK = 7
 
 
 class TuneResult(ctypes.Structure):
@@ -167,6 +169,7 @@ def lib() -> ctypes.CDLL:
             "fk20_pairing_n": ([vp, vp, vp, sz, vp], i),
             "g2p_op_n": ([i, vp, vp, vp, sz, vp], i),
             "fk20_default_release": ([i], i),
+            "fk20_check_status": ([ctypes.POINTER(i)], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

@@ -47,6 +47,7 @@ typedef struct { fp_t x, y, z; } g1p_t;
 #define FK20_ETIMEOUT 1005 /* a persistent launch gave up waiting (results invalid) */
 #define FK20_ETOOBIG 1006  /* request larger than the fixed scratch of a no-allocation entry point */
 #define FK20_EAGAIN 1007   /* server: the request is not finished yet / the queue is full */
+#define FK20_ECHECK 1008   /* checked build: a kernel check stopped a launch (fk20_check_status says which) */
 
 /* ------------------------------------------------------------------ context
  * A context owns, on one device, the fixed-base tables built from xext_fft
@@ -156,6 +157,10 @@ int fk20_ctx_autotune(fk20_ctx *ctx, unsigned n, unsigned rows, size_t max_table
  * 32 GB at w = 13 and 116 GB at w = 15 (9 instead of 10 windows per GLV
  * half). */
 #define FK20_OPT_WINDOW 6
+/* FK20_OPT_TEST_CHECK: for tests of the checked build only -- nonzero makes
+ * the next MSM launches record FK20_CHECK_MSM_PLANTED (the normal build
+ * ignores it). */
+#define FK20_OPT_TEST_CHECK 7
 int fk20_ctx_set(fk20_ctx *ctx, int option, int value);
 int fk20_ctx_get(fk20_ctx *ctx, int option, int *value);
 
@@ -334,6 +339,21 @@ int fk20_poly2h_fft(g1p_t *h_fft, const fr_t *polynomial, const g1p_t *xext_fft,
  * and its tables (117 GB at window 15); the next reference-signature call on
  * that device builds them again.  No call may be in flight on it. */
 int fk20_default_release(int device);
+
+/* No counterpart in the reference (it has no checked build; its debug build
+ * asserts).  In the checked build (libfk20b200_checked.so, `make checked`)
+ * the MSM and the persistent G1 FFT check their task decoding, tile and table
+ * indices and the signed-digit recoding against the sizes they were given;
+ * a failure is recorded, never trapped, and the access skipped.  Waits for
+ * the device, then returns the first failing site since the last call
+ * (FK20_CHECK_* below; 0: none) and clears it; *compiled (if not null) is 1
+ * in the checked build, 0 in the normal one, where nothing is checked. */
+#define FK20_CHECK_MSM_TILE 1     /* MSM: warp outside its segment's tiles */
+#define FK20_CHECK_MSM_CARRY 2    /* MSM: a scalar needs more windows than its table has */
+#define FK20_CHECK_MSM_PLANTED 3  /* MSM: the test hook FK20_OPT_TEST_CHECK */
+#define FK20_CHECK_FFT_TASK 11    /* persistent FFT: task decoded outside its segment */
+#define FK20_CHECK_FFT_PROGRAM 12 /* persistent FFT: twiddle program index out of range */
+int fk20_check_status(int *compiled);
 
 /* fk20_poly2toeplitz_coefficients.cu:25 -- polynomial[rows][4096] -> tc[rows][16][512] */
 int fk20_poly2toeplitz_coefficients(fr_t *toeplitz_coefficients, const fr_t *polynomial, unsigned rows,
