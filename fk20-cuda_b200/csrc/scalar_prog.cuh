@@ -30,7 +30,7 @@ namespace fk {
 constexpr int PROG_POSITIONS = 136;
 constexpr int PROG_WORDS = 1 + PROG_POSITIONS / 4;
 constexpr int PROG_SLOTS = 4;                         // P, 3P, 5P, 7P
-constexpr int PROG_SLOT_WORDS = 36 * PROG_SLOTS + 12 * PROG_SLOTS;  // + beta x of each
+constexpr int PROG_SLOT_WORDS = 36 * PROG_SLOTS + 12;  // (x', y', beta x') of each point, then u
 
 // The executor's scratch: for each thread PROG_SLOT_WORDS 32-bit words at
 // base[0], base[stride], ...  While P, 3P, 5P, 7P are formed, point i is
