@@ -181,12 +181,23 @@ int launch_error(int e) { return e >= 2000 ? FK20_ECHECK : FK20_ETIMEOUT; }
 // release() instead, when the owner is torn down.  Growth is geometric in
 // practice (a larger batch, a longer polynomial), so the kept buffers hold
 // less than the live one.
+// fk20_test_fail_allocations: device allocations still to fail (tests of the
+// out-of-memory paths)
+std::atomic<int> g_fail_allocs{0};
+bool injected_alloc_failure() {
+    int left = g_fail_allocs.load();
+    while (left > 0 && !g_fail_allocs.compare_exchange_weak(left, left - 1)) {
+    }
+    return left > 0;
+}
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
     std::vector<void *> outgrown;
     int reserve(size_t need) {
         if (need <= bytes) return 0;
+        if (injected_alloc_failure()) return FK20_ENOMEM;
         void *q = nullptr;
         if (cudaMalloc(&q, need) != cudaSuccess) {
             cudaGetLastError();
@@ -838,6 +849,12 @@ extern "C" {
 const char *fk20_version(void) { return FK20_VERSION; }
 
 int fk20_default_release(int device) { return release_default(device); }
+
+int fk20_test_fail_allocations(int count) {
+    if (count < 0) return FK20_EINVAL;
+    g_fail_allocs.store(count);
+    return 0;
+}
 
 int fk20_check_status(int *compiled) {
     if (compiled) *compiled = FK_CHECKED;
@@ -1723,7 +1740,7 @@ struct fk20_server {
     std::thread worker;
     // statistics since the last reset
     std::vector<double> lat_ms;
-    uint64_t proofs = 0, packs = 0, pack_rows = 0, rejected = 0, nomem = 0;
+    uint64_t proofs = 0, packs = 0, pack_rows = 0, rejected = 0, nomem = 0, cancelled = 0;
     double sum_wait_ms = 0, sum_enqueue_ms = 0, sum_run_ms = 0;  // where the latency goes
     Clock::time_point first, last;
     bool started = false;
@@ -2069,6 +2086,21 @@ int fk20_server_wait(fk20_server *s, uint64_t ticket, int timeout_ms) {
     return status;
 }
 
+int fk20_server_cancel(fk20_server *s, uint64_t ticket) {
+    if (!s) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->live.count(ticket) || s->finished.count(ticket)) return FK20_EINVAL;
+    for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+        if (it->ticket != ticket) continue;
+        s->queue.erase(it);  // never packed: the worker will not touch its buffers
+        s->finished[ticket] = FK20_ECANCELED;
+        s->cancelled++;
+        s->cv_done.notify_all();
+        return 0;
+    }
+    return FK20_EAGAIN;  // in a pack on the GPU: it completes normally
+}
+
 int fk20_server_get_stats(fk20_server *s, fk20_server_stats *out) {
     if (!s || !out) return FK20_EINVAL;
     std::lock_guard<std::mutex> lk(s->mu);
@@ -2091,6 +2123,7 @@ int fk20_server_get_stats(fk20_server *s, fk20_server_stats *out) {
     st.mean_pack_rows = s->packs ? (double)s->pack_rows / s->packs : 0;
     st.rejected = s->rejected;
     st.nomem = s->nomem;
+    st.cancelled = s->cancelled;
     st.mean_wait_ms = v.empty() ? 0 : s->sum_wait_ms / v.size();
     st.mean_enqueue_ms = s->packs ? s->sum_enqueue_ms / s->packs : 0;
     st.mean_run_ms = s->packs ? s->sum_run_ms / s->packs : 0;
@@ -2102,7 +2135,7 @@ int fk20_server_reset_stats(fk20_server *s) {
     if (!s) return FK20_EINVAL;
     std::lock_guard<std::mutex> lk(s->mu);
     s->lat_ms.clear();
-    s->proofs = s->packs = s->pack_rows = s->rejected = s->nomem = 0;
+    s->proofs = s->packs = s->pack_rows = s->rejected = s->nomem = s->cancelled = 0;
     s->sum_wait_ms = s->sum_enqueue_ms = s->sum_run_ms = 0;
     s->started = false;
     return 0;

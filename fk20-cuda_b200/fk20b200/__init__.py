@@ -42,7 +42,8 @@ ABI_SYMBOLS = (
     "fk20_server_wait", "fk20_server_get_stats", "fk20_server_reset_stats", "fk20_server_destroy",
     "fk20_g1p_compress_n", "fk20_h_fft2proofs", "fk20_ctx_poly2proofs", "fk20_ctx_batch_proofs",
     "fk20_ctx_load_commit", "fk20_ctx_commit", "fk20_pairing_check_n", "fk20_pairing_n", "g2p_op_n",
-    "fk20_ctx_check_proof_multi", "fk20_default_release", "fk20_check_status",
+    "fk20_ctx_check_proof_multi", "fk20_default_release", "fk20_check_status", "fk20_server_cancel",
+    "fk20_test_fail_allocations",
 )
 
 # kernel kinds of the per-launch profiler (FK20_K_* in the header)
@@ -51,6 +52,7 @@ FK20_ETIMEOUT = 1005
 FK20_ETOOBIG = 1006
 FK20_EAGAIN = 1007
 FK20_ECHECK = 1008
+FK20_ECANCELED = 1009
 FK20_OPT_FUSED_FFT = 1
 FK20_OPT_MSM_THREADS = 2
 FK20_OPT_FFT_BLOCKS_PER_SM = 3
@@ -76,6 +78,7 @@ class ServerStats(ctypes.Structure):
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
                 ("max_ms", ctypes.c_double), ("wall_s", ctypes.c_double), ("proofs_per_s", ctypes.c_double),
                 ("mean_pack_rows", ctypes.c_double), ("rejected", ctypes.c_uint64), ("nomem", ctypes.c_uint64),
+                ("cancelled", ctypes.c_uint64),
                 ("mean_wait_ms", ctypes.c_double), ("mean_enqueue_ms", ctypes.c_double),
                 ("mean_run_ms", ctypes.c_double)]
 
@@ -170,6 +173,8 @@ def lib() -> ctypes.CDLL:
             "g2p_op_n": ([i, vp, vp, vp, sz, vp], i),
             "fk20_default_release": ([i], i),
             "fk20_check_status": ([ctypes.POINTER(i)], i),
+            "fk20_server_cancel": ([vp, ctypes.c_uint64], i),
+            "fk20_test_fail_allocations": ([i], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -379,6 +384,13 @@ class Server:
     def wait(self, ticket: int, timeout_ms: int = -1) -> int:
         rc = lib().fk20_server_wait(self.h, ticket, timeout_ms)
         if rc != FK20_EAGAIN:
+            self._held.pop(ticket, None)
+        return rc
+
+    def cancel(self, ticket: int) -> int:
+        """0: cancelled (the buffers are free again); FK20_EAGAIN: already on the GPU."""
+        rc = lib().fk20_server_cancel(self.h, ticket)
+        if rc == 0:
             self._held.pop(ticket, None)
         return rc
 

@@ -48,6 +48,7 @@ typedef struct { fp_t x, y, z; } g1p_t;
 #define FK20_ETOOBIG 1006  /* request larger than the fixed scratch of a no-allocation entry point */
 #define FK20_EAGAIN 1007   /* server: the request is not finished yet / the queue is full */
 #define FK20_ECHECK 1008   /* checked build: a kernel check stopped a launch (fk20_check_status says which) */
+#define FK20_ECANCELED 1009 /* server: the request was cancelled before it was packed */
 
 /* ------------------------------------------------------------------ context
  * A context owns, on one device, the fixed-base tables built from xext_fft
@@ -308,6 +309,7 @@ typedef struct {
     double mean_pack_rows;
     uint64_t rejected; /* submits refused with FK20_EAGAIN (max_queue requests waiting) */
     uint64_t nomem;    /* requests failed with FK20_ENOMEM (too large for the device memory alone) */
+    uint64_t cancelled; /* requests cancelled with fk20_server_cancel before they were packed */
     double mean_wait_ms;    /* submit -> the request's pack is formed (mean over requests) */
     double mean_enqueue_ms; /* host time to stage and enqueue a pack (mean over packs) */
     double mean_run_ms;     /* pack enqueued -> its proofs copied out (mean over packs) */
@@ -320,6 +322,11 @@ int fk20_server_submit(fk20_server *srv, const fr_t *poly, unsigned n, g1p_t *h_
 /* 0: done, result written (the ticket is then forgotten); FK20_EAGAIN: not
  * done within timeout_ms (< 0 waits without limit); else the error of its pack. */
 int fk20_server_wait(fk20_server *srv, uint64_t ticket, int timeout_ms);
+/* Cancels a request that is still waiting for a pack: 0 (its buffers are
+ * free again at once; fk20_server_wait then reports FK20_ECANCELED);
+ * FK20_EAGAIN when it is already in a pack on the GPU (it completes
+ * normally); FK20_EINVAL for an unknown or finished ticket. */
+int fk20_server_cancel(fk20_server *srv, uint64_t ticket);
 int fk20_server_get_stats(fk20_server *srv, fk20_server_stats *stats);
 int fk20_server_reset_stats(fk20_server *srv);
 /* Finishes every submitted request, then stops the worker and frees the slots. */
@@ -354,6 +361,11 @@ int fk20_default_release(int device);
 #define FK20_CHECK_FFT_TASK 11    /* persistent FFT: task decoded outside its segment */
 #define FK20_CHECK_FFT_PROGRAM 12 /* persistent FFT: twiddle program index out of range */
 int fk20_check_status(int *compiled);
+
+/* No counterpart in the reference.  For tests of the out-of-memory paths
+ * only: the next `count` device allocations the library makes fail as if
+ * the device were full (FK20_ENOMEM); 0 ends the injection. */
+int fk20_test_fail_allocations(int count);
 
 /* fk20_poly2toeplitz_coefficients.cu:25 -- polynomial[rows][4096] -> tc[rows][16][512] */
 int fk20_poly2toeplitz_coefficients(fr_t *toeplitz_coefficients, const fr_t *polynomial, unsigned rows,
