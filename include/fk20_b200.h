@@ -425,8 +425,10 @@ int g1p_fft_n(g1p_t *output, const g1p_t *input, unsigned log_m, unsigned count,
  * library holds until exit.  At most 64 transforms (log_m <= 9) per call;
  * more returns FK20_ETOOBIG.  The first call on a device looks up the array's
  * address (under lazy module loading, that is also when the array's memory is
- * committed): make it at start-up, before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race and must be serialised. */
+ * committed): make it at start-up, before any stream capture.  The address
+ * is cached per device for the life of the process: do not reset a device
+ * (cudaDeviceReset) while this entry point is in use.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised. */
 int g1p_fft_noalloc(g1p_t *output, const g1p_t *input, unsigned log_m, unsigned count, int inverse, void *stream);
 
 /* ------------------------------------------------------------------ element-wise helpers
