@@ -65,6 +65,12 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--serve-fft-blocks", type=int, default=0,
                     help="persistent-FFT blocks per SM of each pack (0: adaptive to the backlog)")
+    ap.add_argument("--serve-engine", type=int, default=0,
+                    help="server engine: 0 packs on slots, 1 cohorts (continuous batching at FFT-stage granularity)")
+    ap.add_argument("--serve-cohort-rows", type=int, default=0, help="engine 1: rows per cohort (0 = 64)")
+    ap.add_argument("--serve-cohorts", type=int, default=0, help="engine 1: cohorts in flight (0 = 16)")
+    ap.add_argument("--serve-form-ms", type=int, default=0, help="engine 1: longest partial-group wait (0 = 25)")
+    ap.add_argument("--serve-stages", type=int, default=0, help="engine 1: FFT stages per launch (0 = 3)")
     ap.add_argument("--serve-max-queue", type=int, default=640,
                     help="waiting requests beyond which the server refuses submits with FK20_EAGAIN (overload "
                          "control; the client drops refused requests and counts them)")
@@ -586,7 +592,8 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
     mean_proofs = float((sizes // 8 * weights).sum())
     srv = E.Server(ctx, max_rows=args.serve_max_rows, slots=args.serve_slots, fft_blocks_per_sm=args.serve_fft_blocks,
                    latency_rows=args.serve_latency_rows, burst_rows=args.serve_burst_rows,
-                   max_queue=args.serve_max_queue)
+                   max_queue=args.serve_max_queue, engine=args.serve_engine, cohort_rows=args.serve_cohort_rows,
+                   cohorts=args.serve_cohorts, form_ms=args.serve_form_ms, stages_per_launch=args.serve_stages)
     loads = []
     rng = np.random.default_rng(42)
     check = []  # (n, pool index, output) kept for the bit-exactness check
@@ -653,7 +660,8 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
                       "mean_pack_rows": st["mean_pack_rows"], "packs": st["packs"],
                       # where the latency goes: waiting for a pack, staging it, running it
                       "mean_wait_ms": st["mean_wait_ms"], "mean_enqueue_ms": st["mean_enqueue_ms"],
-                      "mean_run_ms": st["mean_run_ms"],
+                      "mean_run_ms": st["mean_run_ms"], "mean_msm_ms": st["mean_msm_ms"],
+                      "mean_launch_ms": st["mean_launch_ms"], "launches": st["launches"],
                       "errors": sum(1 for r in done_rc if r != 0),
                       # admission: submits refused with FK20_EAGAIN (max_queue requests waiting)
                       "admitted": count - refused, "refused": refused,
@@ -676,6 +684,10 @@ def serve_on(args, ctx, rank, loads_frac, seconds, warmup_s, plain_ms):
                    "latency_rows": args.serve_latency_rows or args.serve_max_rows,
                    "burst_rows": args.serve_burst_rows or min(4096, args.serve_max_rows * 7 // 5),
                    "max_queue": args.serve_max_queue,
+                   "engine": "cohorts" if args.serve_engine == 1 else "packs on slots",
+                   "cohort": {"rows": args.serve_cohort_rows or 64, "in_flight": args.serve_cohorts or 16,
+                              "form_ms": args.serve_form_ms or 25, "stages_per_launch": args.serve_stages or 3}
+                   if args.serve_engine == 1 else None,
                    "arrival_window_s": seconds, "warmup_s_excluded": warmup_s,
                    "table_bytes": ctx.device_bytes()},
         "plain_batch": {"rows": rows, "n": n, "proofs_per_s": plain_pps, "latency_ms": plain_ms},

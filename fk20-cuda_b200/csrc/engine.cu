@@ -1725,10 +1725,44 @@ size_t pack_bytes(const unsigned cnt[3]) {
 
 }  // namespace
 
+namespace {
+// engine 1: buffers of one cohort, sized at creation for cohort_rows rows of
+// the longest length
+struct CohortBuf {
+    DevBuf S, D, ready, dpoly, dout;
+    void *hpoly = nullptr, *hout = nullptr;
+    cudaEvent_t msm_done = nullptr, out_done = nullptr;
+};
+// engine 1: requests of one length admitted together, proved as one segment
+// of the persistent FFT launches; state 0 free, 1 formed and its inputs
+// staged, 5 in the MSM batch, 2 in the FFT launches, 3 output copy enqueued
+struct Cohort {
+    int state = 0;
+    int log_m = 0, rows = 0, G = 0;
+    int stage = 0;       // first FFT stage not yet launched
+    uint64_t order = 0;  // admission order (older cohorts first in a launch)
+    int rc = 0;          // error of enqueueing its work
+    std::vector<Req> reqs;
+    Clock::time_point t_form, t_enq;
+};
+}  // namespace
+
 struct fk20_server {
     fk20_ctx *ctx = nullptr;
     fk20_server_config cfg{};
     std::vector<Slot> slots;
+    // engine 1 (cohorts)
+    std::vector<CohortBuf> cbuf;
+    std::vector<Cohort> cohort;
+    cudaStream_t st_msm = nullptr, st_fft = nullptr;
+    DevBuf hdr;                  // persistent-launch header: task counter at 0, error flag at 128
+    int *iter_err = nullptr;     // pinned copy of the last launch's error flag
+    cudaEvent_t iter_done = nullptr, msm_done = nullptr;
+    bool iter_busy = false, msm_busy = false;
+    uint64_t next_order = 1;
+    Clock::time_point t_launch;  // the FFT launch in flight was enqueued
+    double sum_msm_ms = 0, sum_launch_ms = 0;
+    uint64_t launches = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Req> queue;
@@ -1957,8 +1991,331 @@ void server_main(fk20_server *s) {
     }
 }
 
+// ---------------------------------------------------------------- engine 1: cohorts
+// Continuous batching at FFT-stage granularity.  The waiting requests of one
+// length become a cohort (one segment of up to cohort_rows rows) as soon as a
+// 32-row group is full or the oldest has waited form_ms.  Its inputs are
+// staged and its toeplitz + MSM run on their own stream; once that is done
+// the cohort joins the persistent FFT launches, each of which advances every
+// cohort in flight by stages_per_launch stages (a stage window per segment:
+// the readiness counters and tiles carry over from launch to launch, with the
+// same epoch, so a window's first stage finds its inputs ready).  A cohort
+// whose last stage ran gets its output kernel and copy behind that launch.
+// One FFT launch is in flight at a time; the MSMs of new cohorts run beside
+// it.
+
+// inputs of a formed cohort into its pinned staging (host copies only)
+void cohort_stage(Cohort &c, const CohortBuf &b) {
+    const size_t n = (size_t)8 << c.log_m;
+    for (size_t i = 0; i < c.reqs.size(); i++)
+        memcpy((fr_t *)b.hpoly + i * n, c.reqs[i].poly, n * sizeof(fr_t));
+}
+
+// The new cohorts' inputs, toeplitz + Fr FFTs and ONE MSM launch over all of
+// them, on the MSM stream (beside the FFT launches); `msm_done` follows it.
+int cohort_msm(fk20_server *s, const std::vector<int> &fresh) {
+    fk20_ctx *ctx = s->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t st = s->st_msm;
+    MsmArgs a{};
+    unsigned warps = 0;
+    for (size_t k = 0; k < fresh.size(); k++) {
+        const Cohort &c = s->cohort[fresh[k]];
+        const CohortBuf &b = s->cbuf[fresh[k]];
+        const int m = 1 << c.log_m, n = m * 8;
+        Tables *T = tables_for(ctx, c.log_m);
+        CK(cudaMemcpyAsync(b.dpoly.p, b.hpoly, (size_t)c.rows * n * sizeof(fr_t), cudaMemcpyHostToDevice, st));
+        launch_tc_fft((uint4 *)b.S.p, (const uint64_t *)b.dpoly.p, nullptr, n, c.log_m, (unsigned)c.rows, st);
+        CKL();
+        CK(cudaMemsetAsync(b.ready.p, 0, (size_t)c.G * m * sizeof(unsigned), st));
+        a.seg[k] = MsmSeg{(uint4 *)b.D.p, (const uint4 *)b.S.p, (const uint4 *)T->table.p, c.G, c.log_m, c.rows,
+                          T->cb, T->W, warps};
+        warps += (unsigned)c.G << c.log_m;
+    }
+    a.nseg = (int)fresh.size();
+    a.times_m = 0;
+    a.test_check = ctx->test_check;
+    a.warps = warps;
+    launch_msm(a, ctx->msm_threads, st);
+    CKL();
+    CK(cudaEventRecord(s->msm_done, st));
+    CK(cudaLaunchHostFunc(st, pack_done_cb, s));
+    return 0;
+}
+
+// One persistent FFT launch on the FFT stream that advances every cohort in
+// `act` (oldest first) by up to stages_per_launch stages, then the outputs of
+// the cohorts that finished.
+int cohort_launch(fk20_server *s, const std::vector<int> &act) {
+    fk20_ctx *ctx = s->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t st = s->st_fft;
+    FusedPlan p{};
+    unsigned widest = 0;
+    for (size_t k = 0; k < act.size(); k++) {
+        Cohort &c = s->cohort[act[k]];
+        const CohortBuf &b = s->cbuf[act[k]];
+        const int m = 1 << c.log_m, total = 2 * c.log_m - 1;
+        p.seg[k] = FusedSeg{(uint4 *)b.D.p, (unsigned *)b.ready.p};
+        p.blk.G[k] = c.G;
+        p.blk.log_m[k] = c.log_m;
+        p.blk.s_lo[k] = (unsigned char)c.stage;
+        p.blk.s_hi[k] = (unsigned char)std::min(total, c.stage + (int)s->cfg.stages_per_launch);
+        widest += (unsigned)c.G * (m / 2);
+    }
+    p.blk.nseg = (int)act.size();
+    fused_blocks_build(p.blk);
+    p.next = (unsigned *)s->hdr.p;
+    p.err = (int *)((char *)s->hdr.p + 128);
+    p.epoch = 1;  // fixed for a cohort's life: its counters carry over between launches
+    p.spin_limit = ctx->wait_limit;
+    p.unpublished = ctx->unpublished;
+    const unsigned max_blocks = (widest + FFT_WARPS - 1) / FFT_WARPS;
+    p.blocks = (int)std::min<unsigned>((unsigned)(ctx->sms * ctx->fused_occupancy), max_blocks);
+    CK(cudaMemsetAsync(s->hdr.p, 0, SYNC_HDR, st));
+    launch_g1_fused(p, st);
+    CKL();
+    CK(cudaMemcpyAsync(s->iter_err, p.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    for (size_t k = 0; k < act.size(); k++) {
+        Cohort &c = s->cohort[act[k]];
+        const CohortBuf &b = s->cbuf[act[k]];
+        c.stage = p.blk.s_hi[k];
+        if (c.stage < 2 * c.log_m - 1) continue;
+        const int m = 1 << c.log_m;
+        launch_tile_to_ref((uint64_t *)b.dout.p, (const uint4 *)b.D.p, nullptr, c.rows, c.log_m, 0, st);
+        CKL();
+        CK(cudaMemcpyAsync(b.hout, b.dout.p, (size_t)c.rows * m * sizeof(g1p_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(b.out_done, st));
+        c.state = 3;
+    }
+    CK(cudaEventRecord(s->iter_done, st));
+    CK(cudaLaunchHostFunc(st, pack_done_cb, s));
+    return 0;
+}
+
+// a cohort's requests finish with `status` (caller holds the server lock)
+void cohort_finish(fk20_server *s, Cohort &c, int status, Clock::time_point now) {
+    for (const Req &r : c.reqs) {
+        s->finished[r.ticket] = status;
+        if (!status) {
+            s->lat_ms.push_back(std::chrono::duration<double, std::milli>(now - r.t0).count());
+            s->proofs += r.n / 8;
+        }
+    }
+    s->packs++;
+    s->pack_rows += c.reqs.size();
+    s->sum_run_ms += std::chrono::duration<double, std::milli>(now - c.t_enq).count();
+    s->last = now;
+    c.reqs.clear();
+    c.state = 0;
+    c.rc = 0;
+}
+
+void server_main_cohorts(fk20_server *s) {
+    cudaSetDevice(s->ctx->device);
+    const int NC = (int)s->cohort.size();
+    const int rows_max = (int)s->cfg.cohort_rows;
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        bool progress = false;
+        // 1. the FFT launch in flight
+        if (s->iter_busy) {
+            const cudaError_t q = cudaEventQuery(s->iter_done);
+            if (q != cudaErrorNotReady) {
+                s->iter_busy = false;
+                s->launches++;
+                s->sum_launch_ms += std::chrono::duration<double, std::milli>(Clock::now() - s->t_launch).count();
+                int status = 0;
+                if (q != cudaSuccess) {
+                    cudaGetLastError();
+                    status = (int)q;
+                } else if (*s->iter_err) {
+                    status = launch_error(*s->iter_err);
+                    *s->iter_err = 0;
+                }
+                if (status) {  // every cohort that was in the launch has invalid tiles
+                    const Clock::time_point now = Clock::now();
+                    for (Cohort &c : s->cohort)
+                        if (c.state == 2 || c.state == 3) cohort_finish(s, c, status, now);
+                    s->cv_done.notify_all();
+                }
+                progress = true;
+            }
+        }
+        // 2. outputs copied: hand the proofs to the callers
+        for (int i = 0; i < NC; i++) {
+            Cohort &c = s->cohort[i];
+            if (c.state != 3) continue;
+            const cudaError_t q = cudaEventQuery(s->cbuf[i].out_done);
+            if (q == cudaErrorNotReady) continue;
+            int status = 0;
+            if (q != cudaSuccess) {
+                cudaGetLastError();
+                status = (int)q;
+            }
+            std::vector<Req> done;
+            done.swap(c.reqs);
+            c.state = 4;  // copying out: not free yet
+            lk.unlock();
+            if (!status) {
+                const size_t per = (size_t)(1 << c.log_m);
+                for (size_t k = 0; k < done.size(); k++)
+                    memcpy(done[k].out, (const g1p_t *)s->cbuf[i].hout + k * per, per * sizeof(g1p_t));
+            }
+            const Clock::time_point now = Clock::now();
+            lk.lock();
+            c.reqs.swap(done);
+            cohort_finish(s, c, status, now);
+            s->cv_done.notify_all();
+            progress = true;
+        }
+        // 4. new cohorts: per length (longest first), whole 32-row groups, or
+        // what waits once its oldest request has waited form_ms (or at shutdown)
+        const Clock::time_point now = Clock::now();
+        for (int L = 9; L >= 7 && !s->queue.empty(); L--) {
+            int freei = -1;
+            for (int i = 0; i < NC; i++)
+                if (s->cohort[i].state == 0) {
+                    freei = i;
+                    break;
+                }
+            if (freei < 0) break;
+            size_t count = 0;
+            double oldest_ms = 0;
+            for (const Req &r : s->queue)
+                if (log_m_for_n(r.n) == L) {
+                    if (!count) oldest_ms = std::chrono::duration<double, std::milli>(now - r.t0).count();
+                    count++;
+                }
+            if (!count) continue;
+            const bool late = s->stop || oldest_ms >= (double)s->cfg.form_ms;
+            size_t take = std::min(count, (size_t)rows_max);
+            if (!late) take = take / 32 * 32;
+            if (!take) continue;
+            Cohort &c = s->cohort[freei];
+            c.reqs.clear();
+            std::deque<Req> rest;
+            for (const Req &r : s->queue) {
+                if (c.reqs.size() < take && log_m_for_n(r.n) == L) c.reqs.push_back(r);
+                else rest.push_back(r);
+            }
+            s->queue.swap(rest);
+            c.log_m = L;
+            c.rows = (int)c.reqs.size();
+            c.G = (c.rows + 31) / 32;
+            c.stage = 0;
+            c.order = s->next_order++;
+            c.state = 1;
+            c.t_form = Clock::now();
+            for (const Req &r : c.reqs)
+                s->sum_wait_ms += std::chrono::duration<double, std::milli>(c.t_form - r.t0).count();
+            lk.unlock();
+            cohort_stage(c, s->cbuf[freei]);
+            c.t_enq = Clock::now();
+            lk.lock();
+            s->sum_enqueue_ms += std::chrono::duration<double, std::milli>(c.t_enq - c.t_form).count();
+            progress = true;
+        }
+        // 5. the MSM batch in flight: done -> its cohorts join the FFT launches
+        if (s->msm_busy) {
+            const cudaError_t q = cudaEventQuery(s->msm_done);
+            if (q != cudaErrorNotReady) {
+                s->msm_busy = false;
+                const Clock::time_point t = Clock::now();
+                for (Cohort &c : s->cohort) {
+                    if (c.state != 5) continue;
+                    if (q != cudaSuccess) {
+                        cohort_finish(s, c, (int)q, t);
+                    } else {
+                        c.state = 2;
+                        s->sum_msm_ms += std::chrono::duration<double, std::milli>(t - c.t_enq).count();
+                    }
+                }
+                if (q != cudaSuccess) {
+                    cudaGetLastError();
+                    s->cv_done.notify_all();
+                }
+                progress = true;
+            }
+        }
+        // 6. the next MSM batch: every staged cohort
+        if (!s->msm_busy) {
+            std::vector<int> fresh;
+            for (int i = 0; i < NC; i++)
+                if (s->cohort[i].state == 1) fresh.push_back(i);
+            if (!fresh.empty()) {
+                for (int i : fresh) s->cohort[i].state = 5;
+                s->msm_busy = true;
+                lk.unlock();
+                const int rc = cohort_msm(s, fresh);
+                lk.lock();
+                if (rc) {
+                    s->msm_busy = false;
+                    const Clock::time_point t = Clock::now();
+                    for (int i : fresh) cohort_finish(s, s->cohort[i], rc, t);
+                    s->cv_done.notify_all();
+                }
+                progress = true;
+            }
+        }
+        // 7. the next FFT launch over the cohorts in the FFT stages, oldest first
+        if (!s->iter_busy) {
+            std::vector<int> act;
+            for (int i = 0; i < NC; i++)
+                if (s->cohort[i].state == 2) act.push_back(i);
+            std::sort(act.begin(), act.end(),
+                      [&](int x, int y) { return s->cohort[x].order < s->cohort[y].order; });
+            if (!act.empty()) {
+                s->iter_busy = true;
+                s->t_launch = Clock::now();
+                lk.unlock();
+                const int rc = cohort_launch(s, act);
+                lk.lock();
+                if (rc) {  // nothing of it reached the GPU in a usable state
+                    s->iter_busy = false;
+                    const Clock::time_point t = Clock::now();
+                    for (int i : act) cohort_finish(s, s->cohort[i], rc, t);
+                    s->cv_done.notify_all();
+                }
+                progress = true;
+            }
+        }
+        bool busy = s->iter_busy || s->msm_busy;
+        for (const Cohort &c : s->cohort) busy |= c.state != 0;
+        if (s->stop && s->queue.empty() && !busy) break;
+        if (progress) continue;
+        // sleep until a request arrives or a stream reaches its callback;
+        // bounded, to re-check the formation deadline
+        s->cv_work.wait_for(lk, std::chrono::milliseconds(1), [&] { return s->wake.load() || s->stop; });
+        s->wake.store(false);
+    }
+}
+
 void server_free(fk20_server *s) {
     DeviceGuard dg(s->ctx->device);
+    if (s->st_msm) cudaStreamSynchronize(s->st_msm);
+    if (s->st_fft) cudaStreamSynchronize(s->st_fft);
+    for (CohortBuf &b : s->cbuf) {
+        b.S.release();
+        b.D.release();
+        b.ready.release();
+        b.dpoly.release();
+        b.dout.release();
+        if (b.hpoly) cudaFreeHost(b.hpoly);
+        if (b.hout) cudaFreeHost(b.hout);
+        if (b.msm_done) cudaEventDestroy(b.msm_done);
+        if (b.out_done) cudaEventDestroy(b.out_done);
+    }
+    s->cbuf.clear();
+    s->hdr.release();
+    if (s->iter_err) cudaFreeHost(s->iter_err);
+    if (s->iter_done) cudaEventDestroy(s->iter_done);
+    if (s->msm_done) cudaEventDestroy(s->msm_done);
+    if (s->st_msm) cudaStreamDestroy(s->st_msm);
+    if (s->st_fft) cudaStreamDestroy(s->st_fft);
+    s->iter_err = nullptr;
+    s->iter_done = s->msm_done = nullptr;
+    s->st_msm = s->st_fft = nullptr;
     for (Slot &sl : s->slots) {
         if (sl.st) cudaStreamSynchronize(sl.st);
         sl.ws.release();
@@ -1987,8 +2344,61 @@ int fk20_server_create(fk20_server **out, fk20_ctx *ctx, const fk20_server_confi
     if (c.max_rows > 4096 || c.slots > 8) return FK20_EINVAL;
     if (!c.burst_rows) c.burst_rows = std::min(4096u, c.max_rows + c.max_rows * 2 / 5);
     if (c.burst_rows < c.max_rows || c.burst_rows > 4096) return FK20_EINVAL;
+    if (c.engine > 1) return FK20_EINVAL;
+    if (!c.cohort_rows) c.cohort_rows = 64;
+    if (!c.cohorts) c.cohorts = 16;
+    if (!c.form_ms) c.form_ms = 25;
+    if (!c.stages_per_launch) c.stages_per_launch = 3;
+    if (c.cohort_rows < 32 || c.cohort_rows > 256 || c.cohorts > (unsigned)MAX_SEGS || c.stages_per_launch > 17)
+        return FK20_EINVAL;
     fk20_server *s = new fk20_server();
     s->ctx = ctx;
+    if (c.engine == 1) {
+        // cohort buffers for cohort_rows rows of the longest length, all at creation
+        DeviceGuard dg(ctx->device);
+        int rc = 0;
+        const int m = 512, n = 4096, G = (int)((c.cohort_rows + 31) / 32);
+        s->cbuf.resize(c.cohorts);
+        s->cohort.resize(c.cohorts);
+        if (cudaStreamCreateWithFlags(&s->st_msm, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&s->st_fft, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->iter_done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->msm_done, cudaEventDisableTiming) != cudaSuccess)
+            rc = (int)cudaGetLastError();
+        if (!rc && cudaMallocHost(&s->iter_err, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            rc = FK20_ENOMEM;
+        }
+        if (!rc) {
+            *s->iter_err = 0;
+            rc = s->hdr.reserve(SYNC_HDR);
+        }
+        for (CohortBuf &b : s->cbuf) {
+            if (rc) break;
+            const size_t in_b = (size_t)c.cohort_rows * n * sizeof(fr_t), out_b = (size_t)c.cohort_rows * m * sizeof(g1p_t);
+            rc = b.S.reserve(scal_bytes(G, m));
+            if (!rc) rc = b.D.reserve(tile_bytes(G, m));
+            if (!rc) rc = b.ready.reserve((size_t)G * m * sizeof(unsigned));
+            if (!rc) rc = b.dpoly.reserve(in_b);
+            if (!rc) rc = b.dout.reserve(out_b);
+            if (!rc && (cudaMallocHost(&b.hpoly, in_b) != cudaSuccess || cudaMallocHost(&b.hout, out_b) != cudaSuccess)) {
+                cudaGetLastError();
+                rc = FK20_ENOMEM;
+            }
+            if (!rc && (cudaEventCreateWithFlags(&b.msm_done, cudaEventDisableTiming) != cudaSuccess ||
+                        cudaEventCreateWithFlags(&b.out_done, cudaEventDisableTiming) != cudaSuccess))
+                rc = (int)cudaGetLastError();
+        }
+        if (rc) {
+            server_free(s);
+            delete s;
+            return rc;
+        }
+        s->cfg = c;
+        s->worker = std::thread(server_main_cohorts, s);
+        *out = s;
+        return 0;
+    }
     {
         DeviceGuard dg(ctx->device);
         if (!c.hbm_budget) {
@@ -2127,6 +2537,9 @@ int fk20_server_get_stats(fk20_server *s, fk20_server_stats *out) {
     st.mean_wait_ms = v.empty() ? 0 : s->sum_wait_ms / v.size();
     st.mean_enqueue_ms = s->packs ? s->sum_enqueue_ms / s->packs : 0;
     st.mean_run_ms = s->packs ? s->sum_run_ms / s->packs : 0;
+    st.mean_msm_ms = s->packs ? s->sum_msm_ms / s->packs : 0;
+    st.mean_launch_ms = s->launches ? s->sum_launch_ms / s->launches : 0;
+    st.launches = s->launches;
     *out = st;
     return 0;
 }
@@ -2136,7 +2549,8 @@ int fk20_server_reset_stats(fk20_server *s) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->lat_ms.clear();
     s->proofs = s->packs = s->pack_rows = s->rejected = s->nomem = s->cancelled = 0;
-    s->sum_wait_ms = s->sum_enqueue_ms = s->sum_run_ms = 0;
+    s->sum_wait_ms = s->sum_enqueue_ms = s->sum_run_ms = s->sum_msm_ms = s->sum_launch_ms = 0;
+    s->launches = 0;
     s->started = false;
     return 0;
 }

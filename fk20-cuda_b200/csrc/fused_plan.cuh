@@ -16,7 +16,7 @@
 
 namespace fk {
 
-constexpr int MAX_SEGS = 8;
+constexpr int MAX_SEGS = 24;
 constexpr int FUSED_MAX_LOG_M = 9;
 constexpr int MAX_FUSED_STAGES = 2 * FUSED_MAX_LOG_M - 1;
 constexpr int MAX_FUSED_BLOCKS = MAX_SEGS * MAX_FUSED_STAGES;
@@ -26,19 +26,34 @@ struct FusedBlocks {
     unsigned char seg[MAX_FUSED_BLOCKS], stage[MAX_FUSED_BLOCKS];
     int nblk;
     int G[MAX_SEGS], log_m[MAX_SEGS];
+    // stage window [s_lo, s_hi) of each segment; s_hi = 0 means all its
+    // stages.  A segment whose window starts above stage 0 continues the
+    // stages an earlier launch ran on the same tiles and readiness counters
+    // (counters kept, same epoch), so its first stage finds its inputs ready.
+    unsigned char s_lo[MAX_SEGS], s_hi[MAX_SEGS];
     int nseg;
 };
 
+FK_HD int fused_stage_hi(const FusedBlocks &b, int k) { return b.s_hi[k] ? b.s_hi[k] : 2 * b.log_m[k] - 1; }
+
 // fills start/seg/stage from G, log_m, nseg; returns the task count
+// Blocks go in order of the stage RELATIVE to each segment's window (its
+// first stage in this launch, then its second, ...): segments whose windows
+// start at different stages then progress side by side, and a launch lasts
+// about as many task times as its longest window, not the span of all
+// windows.  A task of relative stage r only reads what tasks of relative
+// stage r - 1 of its own segment (lower task indices) or an earlier launch
+// wrote.
 FK_HD unsigned fused_blocks_build(FusedBlocks &b) {
-    int maxst = 0;
+    int maxw = 0;
     for (int k = 0; k < b.nseg; k++)
-        if (2 * b.log_m[k] - 1 > maxst) maxst = 2 * b.log_m[k] - 1;
+        if (fused_stage_hi(b, k) - b.s_lo[k] > maxw) maxw = fused_stage_hi(b, k) - b.s_lo[k];
     unsigned task = 0;
     int nb = 0;
-    for (int S = 0; S < maxst; S++)
+    for (int r = 0; r < maxw; r++)
         for (int k = 0; k < b.nseg; k++) {
-            if (S >= 2 * b.log_m[k] - 1) continue;
+            const int S = b.s_lo[k] + r;
+            if (S >= fused_stage_hi(b, k)) continue;
             b.start[nb] = task;
             b.seg[nb] = (unsigned char)k;
             b.stage[nb] = (unsigned char)S;

@@ -70,7 +70,9 @@ class TuneResult(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("max_rows", ctypes.c_uint), ("slots", ctypes.c_uint), ("hbm_budget", ctypes.c_size_t),
                 ("max_queue", ctypes.c_uint), ("fft_blocks_per_sm", ctypes.c_uint),
-                ("latency_rows", ctypes.c_uint), ("burst_rows", ctypes.c_uint)]
+                ("latency_rows", ctypes.c_uint), ("burst_rows", ctypes.c_uint), ("engine", ctypes.c_uint),
+                ("cohort_rows", ctypes.c_uint), ("cohorts", ctypes.c_uint), ("form_ms", ctypes.c_uint),
+                ("stages_per_launch", ctypes.c_uint)]
 
 
 class ServerStats(ctypes.Structure):
@@ -80,7 +82,8 @@ class ServerStats(ctypes.Structure):
                 ("mean_pack_rows", ctypes.c_double), ("rejected", ctypes.c_uint64), ("nomem", ctypes.c_uint64),
                 ("cancelled", ctypes.c_uint64),
                 ("mean_wait_ms", ctypes.c_double), ("mean_enqueue_ms", ctypes.c_double),
-                ("mean_run_ms", ctypes.c_double)]
+                ("mean_run_ms", ctypes.c_double), ("mean_msm_ms", ctypes.c_double),
+                ("mean_launch_ms", ctypes.c_double), ("launches", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -365,8 +368,10 @@ class Server:
     output (n/8 x 18 uint64); both are kept referenced until wait()."""
 
     def __init__(self, ctx: Context, max_rows: int = 0, slots: int = 0, hbm_budget: int = 0, max_queue: int = 0,
-                 fft_blocks_per_sm: int = 0, latency_rows: int = 0, burst_rows: int = 0):
-        cfg = ServerConfig(max_rows, slots, hbm_budget, max_queue, fft_blocks_per_sm, latency_rows, burst_rows)
+                 fft_blocks_per_sm: int = 0, latency_rows: int = 0, burst_rows: int = 0, engine: int = 0,
+                 cohort_rows: int = 0, cohorts: int = 0, form_ms: int = 0, stages_per_launch: int = 0):
+        cfg = ServerConfig(max_rows, slots, hbm_budget, max_queue, fft_blocks_per_sm, latency_rows, burst_rows,
+                           engine, cohort_rows, cohorts, form_ms, stages_per_launch)
         h = ctypes.c_void_p()
         call("fk20_server_create", ctypes.byref(h), ctx.h, ctypes.byref(cfg))
         self.h = h

@@ -300,6 +300,17 @@ typedef struct {
                                    length (0 = max_rows; <= max_rows) */
     unsigned burst_rows;        /* pack size while more than 2 max_rows requests wait: larger packs drain a
                                    backlog faster (0 = 7/5 max_rows, i.e. 224 for 160; max_rows..4096) */
+    unsigned engine;            /* 0: packs on slots (above).  1: cohorts -- continuous batching at FFT-stage
+                                   granularity: the waiting requests of one length form a cohort as soon as a
+                                   32-row group is full or the oldest has waited form_ms; its toeplitz + MSM
+                                   run on their own stream, and every persistent-FFT launch advances all
+                                   cohorts in flight by stages_per_launch stages, so a new cohort joins the
+                                   next launch instead of waiting for a slot.  max_rows, slots, latency_rows,
+                                   burst_rows and fft_blocks_per_sm apply to engine 0 only. */
+    unsigned cohort_rows;       /* engine 1: rows per cohort at most (32..256; 0 = 64) */
+    unsigned cohorts;           /* engine 1: cohorts in flight at most (1..24; 0 = 16) */
+    unsigned form_ms;           /* engine 1: longest wait before a partial 32-row group is proved (0 = 25) */
+    unsigned stages_per_launch; /* engine 1: FFT stages per persistent launch (1..17; 0 = 3) */
 } fk20_server_config;
 typedef struct {
     uint64_t requests, proofs, packs;
@@ -313,6 +324,9 @@ typedef struct {
     double mean_wait_ms;    /* submit -> the request's pack is formed (mean over requests) */
     double mean_enqueue_ms; /* host time to stage and enqueue a pack (mean over packs) */
     double mean_run_ms;     /* pack enqueued -> its proofs copied out (mean over packs) */
+    double mean_msm_ms;     /* engine 1: cohort staged -> the iteration with its MSM enqueued (mean over cohorts) */
+    double mean_launch_ms;  /* engine 1: one FFT launch, enqueued -> done (mean over launches) */
+    uint64_t launches;      /* engine 1: FFT launches */
 } fk20_server_stats;
 int fk20_server_create(fk20_server **srv, fk20_ctx *ctx, const fk20_server_config *cfg);
 /* poly: HOST array of n fr_t (n in 1024, 2048, 4096); h_fft: HOST array of

@@ -110,8 +110,28 @@ extern "C" {
 // The persistent G1 FFT's task schedule for nseg segments (G[k] row groups,
 // FFT size 2^log_m[k]): writes each task's (seg, stage, g, i0, i1, tix, kind)
 // as 7 ints and returns the task count (-1 if it exceeds cap).
+// a launch whose segments run only the stages [s_lo, s_hi) (s_hi = 0: all)
+long emul_fused_schedule_w(int nseg, const int *G, const int *log_m, const int *s_lo, const int *s_hi, int *out,
+                           long cap) {
+    FusedBlocks b{};
+    b.nseg = nseg;
+    for (int k = 0; k < nseg; k++) {
+        b.G[k] = G[k], b.log_m[k] = log_m[k];
+        b.s_lo[k] = (unsigned char)s_lo[k], b.s_hi[k] = (unsigned char)s_hi[k];
+    }
+    const unsigned total = fused_blocks_build(b);
+    if ((long)total > cap) return -1;
+    for (unsigned t = 0; t < total; t++) {
+        FusedTask f;
+        fused_task_decode(f, b, t);
+        int *o = out + 7 * (size_t)t;
+        o[0] = f.seg; o[1] = f.S; o[2] = f.g; o[3] = f.i0; o[4] = f.i1; o[5] = f.tix; o[6] = f.kind;
+    }
+    return (long)total;
+}
+
 long emul_fused_schedule(int nseg, const int *G, const int *log_m, int *out, long cap) {
-    FusedBlocks b;
+    FusedBlocks b{};
     b.nseg = nseg;
     for (int k = 0; k < nseg; k++) b.G[k] = G[k], b.log_m[k] = log_m[k];
     const unsigned total = fused_blocks_build(b);

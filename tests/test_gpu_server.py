@@ -21,8 +21,11 @@ def served_ctx(engine):
     c.close()
 
 
-@pytest.mark.parametrize("mode", [{}, {"latency_rows": 4}, {"fft_blocks_per_sm": 1}],
-                         ids=["adaptive", "latency-rows-4", "one-fft-block-per-sm"])
+@pytest.mark.parametrize("mode", [{}, {"latency_rows": 4}, {"fft_blocks_per_sm": 1}, {"engine": 1},
+                                  {"engine": 1, "cohort_rows": 32, "stages_per_launch": 1, "form_ms": 2},
+                                  {"engine": 1, "cohort_rows": 128, "stages_per_launch": 17, "cohorts": 3}],
+                         ids=["adaptive", "latency-rows-4", "one-fft-block-per-sm", "cohorts",
+                              "cohorts-1-stage-per-launch", "cohorts-whole-fft-per-launch"])
 def test_server_results_same_alone_and_in_the_mix(engine, served_ctx, mode):
     """Latency-mode packs (the whole queue, the whole GPU) and throughput-mode
     packs (whole 32-row groups, the SMs split between slots) both occur here:
@@ -42,7 +45,9 @@ def test_server_results_same_alone_and_in_the_mix(engine, served_ctx, mode):
         assert srv.wait(t, max(1, int(1000 * (deadline - time.time())))) == 0
     st = srv.stats()
     assert st["requests"] == len(sizes) and st["proofs"] == sum(n // 8 for n in sizes)
-    assert st["packs"] >= len(sizes) // 16 and 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
+    # engine 0: packs of at most 16 requests; engine 1: at least one cohort per length
+    assert st["packs"] >= (3 if mode.get("engine") else len(sizes) // 16)
+    assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
     srv.close()
     # each result equals that polynomial proved alone
     for j, n in enumerate(sizes):

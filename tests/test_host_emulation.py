@@ -163,6 +163,79 @@ def test_fused_fft_schedule(emul, G, log_m):
             assert vals[(k, g)] == fwd, (k, g)
 
 
+def test_fused_fft_schedule_in_stage_windows(emul):
+    """The server's cohort engine runs each segment's 17 (15, 13) stages over
+    several launches, each launch a stage window per segment, windows of
+    different segments starting at different stages.  Replayed launch by
+    launch on Fr values: inside a launch every task depends only on tasks of
+    lower index or on an earlier launch, the task order keeps windows of
+    different segments side by side (relative stage first), and the result
+    is FFT(upper half zeroed(IFFT)) per segment, as with one launch."""
+    f = emul.emul_fused_schedule_w
+    f.restype = ctypes.c_long
+    R = O.R
+    w512 = O.root_of_unity(512)
+    rng = np.random.default_rng(9)
+    G, log_m = [1, 2, 1], [9, 8, 7]
+    total = [2 * l - 1 for l in log_m]
+    # staggered windows: segment k starts k launches late, 3 stages a launch
+    vals = {(k, g): [int(x) % R for x in rng.integers(0, 2**62, 1 << L)]
+            for k, (gc, L) in enumerate(zip(G, log_m)) for g in range(gc)}
+    start = {key: list(v) for key, v in vals.items()}
+    done = [-3 * k for k in range(3)]  # stages run so far (negative: not started)
+    launches = 0
+    while any(d < t for d, t in zip(done, total)):
+        segs = [k for k in range(3) if 0 <= done[k] < total[k]]
+        lo = [done[k] for k in segs]
+        hi = [min(total[k], done[k] + 3) for k in segs]
+        if segs:
+            nseg = len(segs)
+            cap = sum(G[k] * (1 << log_m[k]) // 2 * (h - l) for k, l, h in zip(segs, lo, hi))
+            out = np.zeros((cap, 7), np.int32)
+            ci = lambda a: (ctypes.c_int * nseg)(*a)
+            n = f(nseg, ci([G[k] for k in segs]), ci([log_m[k] for k in segs]), ci(lo), ci(hi),
+                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.c_long(cap))
+            assert n == cap
+            writer = {}
+            rel_prev = -1
+            for t, (j, S, g, i0, i1, tix, kind) in enumerate(out.tolist()):
+                k = segs[j]
+                rel = S - lo[j]
+                assert lo[j] <= S < hi[j] and rel >= rel_prev  # relative stage never goes back
+                rel_prev = rel
+                for p in (i0, i1):
+                    if S > lo[j]:  # produced in this launch by the previous stage, at a lower index
+                        st, idx = writer[(k, g, p)]
+                        assert st == S - 1 and idx < t
+                    writer[(k, g, p)] = (S, t)
+                v = vals[(k, g)]
+                wt = pow(w512, tix, R)
+                u, x = v[i0], v[i1]
+                if kind == 0:
+                    v[i0], v[i1] = (u + x) % R, (u - x) * wt % R
+                elif kind == 2:
+                    v[i0] = v[i1] = (u + x) % R
+                else:
+                    x = x * wt % R
+                    v[i0], v[i1] = (u + x) % R, (u - x) % R
+            for j, k in enumerate(segs):
+                done[k] = hi[j]
+        for k in range(3):
+            if done[k] < 0:
+                done[k] += 3 if done[k] < 0 else 0
+        launches += 1
+    assert launches >= 7
+    for k, (g_cnt, L) in enumerate(zip(G, log_m)):
+        m = 1 << L
+        wp = [pow(w512, (512 // m) * e, R) for e in range(m)]
+        for g in range(g_cnt):
+            x = start[(k, g)]
+            inv = [sum(x[j] * wp[(-i * j) % m] for j in range(m)) % R for i in range(m)]
+            inv[m // 2:] = [0] * (m // 2)
+            fwd = [sum(inv[j] * wp[(i * j) % m] for j in range(m)) % R for i in range(m)]
+            assert vals[(k, g)] == fwd, (k, g)
+
+
 LAMBDA = 0xAC45A4010001A40200000000FFFFFFFF  # phi = [lambda] on G1, lambda^2 + lambda + 1 = r
 
 
