@@ -308,12 +308,12 @@ struct Profiler {
     nvtxRangeId_t nvtx = 0;
     struct Rec {
         int kind;
-        double products;
+        double products, executed;
         cudaEvent_t a, b;
     };
     std::vector<Rec> pending;
     std::vector<cudaEvent_t> pool;
-    double ms[FK20_NKINDS] = {0}, products[FK20_NKINDS] = {0};
+    double ms[FK20_NKINDS] = {0}, products[FK20_NKINDS] = {0}, executed[FK20_NKINDS] = {0};
     long launches[FK20_NKINDS] = {0};
     cudaEvent_t get() {
         if (!pool.empty()) {
@@ -325,10 +325,11 @@ struct Profiler {
         cudaEventCreate(&e);
         return e;
     }
-    void begin(int kind, double prod, cudaStream_t st) {
+    // `alg` algorithmic and `exe` executed limb products of the launch
+    void begin(int kind, double alg, double exe, cudaStream_t st) {
         if (nvtx_on()) nvtx = nvtxRangeStartA(NVTX_STAGE[kind]);
         if (!on) return;
-        Rec r{kind, prod, get(), get()};
+        Rec r{kind, alg, exe, get(), get()};
         cudaEventRecord(r.a, st);
         pending.push_back(r);
     }
@@ -347,6 +348,7 @@ struct Profiler {
             cudaEventElapsedTime(&t, r.a, r.b);
             ms[r.kind] += t;
             products[r.kind] += r.products;
+            executed[r.kind] += r.executed;
             launches[r.kind] += 1;
             pool.push_back(r.a);
             pool.push_back(r.b);
@@ -355,7 +357,7 @@ struct Profiler {
     }
     void reset() {
         collect();
-        for (int k = 0; k < FK20_NKINDS; k++) ms[k] = products[k] = 0, launches[k] = 0;
+        for (int k = 0; k < FK20_NKINDS; k++) ms[k] = products[k] = executed[k] = 0, launches[k] = 0;
     }
     ~Profiler() {
         for (Rec &r : pending) pool.push_back(r.a), pool.push_back(r.b);
@@ -404,31 +406,54 @@ struct DeviceGuard {  // make ctx->device current for the duration of a call
     }
 };
 
-// ---- algorithmic work model (limb products) ----------------------------------
-// An Fp product is 300 limb products (12-limb CIOS: 144 + 156), an Fp square
-// 234 (the triangular square: 78 + 156), an Fr product 136.  Per operation:
-// complete projective addition 12 M, doubling 6 M + 2 S; the MSM's mixed
-// addition into an XYZZ accumulator 8 M + 2 S.
-constexpr double MP = 300.0, MS = 234.0, MR = 136.0, ADD_P = 12 * MP, MADD_P = 8 * MP + 2 * MS,
-                 DBL_P = 6 * MP + 2 * MS;
+// ---- work model (limb products) -----------------------------------------------
+// Two accountings of each launch, both in 32x32->64-bit limb products.
+//
+// Algorithmic (`alg`): the fixed unit costs of the FK20 work, independent of
+// the formulas a kernel uses -- an Fp product or square 300 limb products
+// (12-limb CIOS: 2 x 12^2 + 12), an Fr product 136; a G1 addition 12, mixed
+// addition 11 and doubling 8 Fp products (the complete projective formulas
+// of Renes-Costello-Batina, a = 0); a fixed-scalar multiplication costs its
+// chain's doublings and additions at those prices.  This is the work that
+// the roofline fraction divides by.
+//
+// Executed (`exe`): the products the kernels actually run with their cheaper
+// formulas -- a triangular square 234 (78 + 156), the MSM's mixed addition
+// into an XYZZ accumulator 8 M + 2 S, the twiddle programs' Jacobian
+// doublings and mixed additions on the isomorphic curve (below).
+constexpr double MP = 300.0, MR = 136.0, ADD_P = 12 * MP;
+constexpr double MADD_A = 11 * MP, DBL_A = 8 * MP;
+constexpr double MS_X = 234.0, MADD_X = 8 * MP + 2 * MS_X, DBL_X = 6 * MP + 2 * MS_X;
 
-// A twiddle program (scalar_prog.cuh): P to Jacobian (2 M + 1 S), 2P with P
-// on its Z (2 M + 5 S), 3P, 5P, 7P by co-Z additions (3 x (5 M + 2 S)), the
-// points brought onto one Z (11 M + 3 S) with their phi images (4 M), the
-// result brought back (3 M + 1 S): 37 M + 16 S; then Jacobian doublings
-// (2 M + 5 S) and mixed additions (8 M + 3 S) for the digits (program_cost
-// counts the precompute's doubling and three additions with them).
-double prog_products(int idx) {
+struct Work {
+    double alg = 0, exe = 0;
+    Work() = default;
+    Work(double a, double e) : alg(a), exe(e) {}
+    explicit Work(double both) : alg(both), exe(both) {}
+    Work &operator+=(const Work &o) { alg += o.alg, exe += o.exe; return *this; }
+    Work operator*(double k) const { return Work(alg * k, exe * k); }
+    Work operator+(const Work &o) const { return Work(alg + o.alg, exe + o.exe); }
+};
+
+// A twiddle program (scalar_prog.cuh).  Algorithmic: its chain's doublings
+// and additions (program_cost counts the 3P, 5P, 7P precompute's doubling and
+// three additions with the digits') plus phi(P).  Executed: P to Jacobian
+// (2 M + 1 S), 2P with P on its Z (2 M + 5 S), 3P, 5P, 7P by co-Z additions
+// (3 x (5 M + 2 S)), the points brought onto one Z (11 M + 3 S) with their
+// phi images (4 M), the result brought back (3 M + 1 S): 37 M + 16 S; then
+// Jacobian doublings (2 M + 5 S) and mixed additions (8 M + 3 S).
+Work prog_products(int idx) {
     const HostConsts &hc = host_consts();
-    if (hc.prog[idx][0] & 0x300u) return 0.0;
-    return 37.0 * MP + 16.0 * MS + (hc.prog_dbl[idx] - 1) * (2 * MP + 5 * MS) +
-           (hc.prog_add[idx] - 3) * (8 * MP + 3 * MS);
+    if (hc.prog[idx][0] & 0x300u) return Work();
+    const double dbl = hc.prog_dbl[idx], add = hc.prog_add[idx];
+    return Work(dbl * DBL_A + add * ADD_P + MP,
+                37.0 * MP + 16.0 * MS_X + (dbl - 1) * (2 * MP + 5 * MS_X) + (add - 3) * (8 * MP + 3 * MS_X));
 }
 
 // one stage over `rows` rows: kind 0 DIF inverse, 1 DIT forward
-double stage_products(int rows, int log_m, int s, int kind) {
+Work stage_products(int rows, int log_m, int s, int kind) {
     const int m = 1 << log_m;
-    double per_row = 0;
+    Work per_row;
     for (int b = 0; b < m / 2; b++) {
         int tix;
         if (kind == 0) {
@@ -438,14 +463,22 @@ double stage_products(int rows, int log_m, int s, int kind) {
             const int half = 1 << s, j = b & (half - 1);
             tix = (j << (log_m - 1 - s)) << (MAX_LOG_M - log_m);
         }
-        per_row += 2 * ADD_P + (tix ? prog_products(tix) : 0.0);
+        per_row += Work(2 * ADD_P) + (tix ? prog_products(tix) : Work());
     }
     return per_row * rows;
 }
 
-double fr_fft_products(int log_m) {  // nontrivial twiddle products of one Fr FFT-m
+Work fr_fft_products(int log_m) {  // nontrivial twiddle products of one Fr FFT-m
     const int m = 1 << log_m;
-    return ((double)log_m * (m / 2) - (m - 1)) * MR;
+    return Work(((double)log_m * (m / 2) - (m - 1)) * MR);
+}
+
+// the fixed-base MSM per output point: 16 terms x 2W window additions (W
+// windows on each GLV half), phi once, and (times_m) log_m doublings
+Work msm_products(int W, int log_m, bool times_m) {
+    Work w(L_COLS * 2 * W * MADD_A + MP, L_COLS * 2 * W * MADD_X + MP);
+    if (times_m) w += Work(log_m * DBL_A, log_m * DBL_X);
+    return w;
 }
 
 // inverse DIF stages 0..L-2, middle (last inverse + zero upper half + first
@@ -453,17 +486,20 @@ double fr_fft_products(int log_m) {  // nontrivial twiddle products of one Fr FF
 int run_hext_to_hfft(Profiler &pf, uint4 *D, int G, int rows, int log_m, int scale, cudaStream_t st) {
     const int m = 1 << log_m;
     for (int s = 0; s < log_m - 1; s++) {
-        pf.begin(FK20_K_STAGE_INV, stage_products(rows, log_m, s, 0), st);
+        const Work w = stage_products(rows, log_m, s, 0);
+        pf.begin(FK20_K_STAGE_INV, w.alg, w.exe, st);
         launch_g1_stage(D, G, log_m, s, 0, st);
         pf.end(st);
         CKL();
     }
-    pf.begin(FK20_K_MIDDLE, (double)rows * (m / 2) * (ADD_P + (scale ? prog_products(512 + log_m) : 0.0)), st);
+    const Work mid = (Work(ADD_P) + (scale ? prog_products(512 + log_m) : Work())) * ((double)rows * (m / 2));
+    pf.begin(FK20_K_MIDDLE, mid.alg, mid.exe, st);
     launch_g1_middle(D, G, log_m, scale, st);
     pf.end(st);
     CKL();
     for (int s = 1; s < log_m; s++) {
-        pf.begin(FK20_K_STAGE_FWD, stage_products(rows, log_m, s, 1), st);
+        const Work w = stage_products(rows, log_m, s, 1);
+        pf.begin(FK20_K_STAGE_FWD, w.alg, w.exe, st);
         launch_g1_stage(D, G, log_m, s, 1, st);
         pf.end(st);
         CKL();
@@ -473,7 +509,7 @@ int run_hext_to_hfft(Profiler &pf, uint4 *D, int G, int rows, int log_m, int sca
 
 int output_launch(Profiler &pf, uint64_t *dst, const uint4 *D, const size_t *row_off, int rows, int log_m,
                   int bitrev_out, cudaStream_t st) {
-    pf.begin(FK20_K_OUTPUT, (double)rows * (1 << log_m) * 3 * MP, st);
+    pf.begin(FK20_K_OUTPUT, (double)rows * (1 << log_m) * 3 * MP, (double)rows * (1 << log_m) * 3 * MP, st);
     launch_tile_to_ref(dst, D, row_off, rows, log_m, bitrev_out, st);
     pf.end(st);
     CKL();
@@ -551,9 +587,8 @@ int msm_launch(fk20_ctx *ctx, Tables *T, uint4 *D, const uint4 *S, int G, int ro
     a.times_m = times_m;
     a.test_check = ctx->test_check;
     a.warps = (unsigned)G << T->log_m;
-    const double prod = (double)rows * (1 << T->log_m) * (L_COLS * 2 * T->W * MADD_P + MP) +
-                        (times_m ? (double)rows * (1 << T->log_m) * T->log_m * DBL_P : 0.0);
-    ctx->prof.begin(FK20_K_MSM, prod, st);
+    const Work w = msm_products(T->W, T->log_m, times_m != 0) * ((double)rows * (1 << T->log_m));
+    ctx->prof.begin(FK20_K_MSM, w.alg, w.exe, st);
     launch_msm(a, ctx->msm_threads, st);
     ctx->prof.end(st);
     CKL();
@@ -625,14 +660,15 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
     const size_t U = sizeof(uint4);
     for (int k = 0; k < nseg; k++) {
         Tables *T = tables_for(ctx, sg[k].log_m);
-        ctx->prof.begin(FK20_K_TC_FFT, (double)sg[k].rows * L_COLS * fr_fft_products(sg[k].log_m), st);
+        const Work w = fr_fft_products(sg[k].log_m) * ((double)sg[k].rows * L_COLS);
+        ctx->prof.begin(FK20_K_TC_FFT, w.alg, w.exe, st);
         launch_tc_fft(S + lay.s_off[k] / U, (const uint64_t *)polys, sg[k].poly_off, (int)T->n, sg[k].log_m,
                       sg[k].rows, st);
         ctx->prof.end(st);
         CKL();
     }
     MsmArgs a{};
-    double prod = 0;
+    Work prod;
     unsigned warps = 0;
     for (int k = 0; k < nseg; k++) {
         Tables *T = tables_for(ctx, sg[k].log_m);
@@ -640,21 +676,20 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
         a.seg[k] = MsmSeg{D + lay.d_off[k] / U, S + lay.s_off[k] / U, (const uint4 *)T->table.p, G, sg[k].log_m,
                           (int)sg[k].rows, T->cb, T->W, warps};
         warps += (unsigned)G * m;
-        prod += (double)sg[k].rows * m * (L_COLS * 2 * T->W * MADD_P + MP) +
-                (full ? 0.0 : (double)sg[k].rows * m * sg[k].log_m * DBL_P);
+        prod += msm_products(T->W, sg[k].log_m, !full) * ((double)sg[k].rows * m);
     }
     a.nseg = nseg;
     a.times_m = full ? 0 : 1;
     a.test_check = ctx->test_check;
     a.warps = warps;
-    ctx->prof.begin(FK20_K_MSM, prod, st);
+    ctx->prof.begin(FK20_K_MSM, prod.alg, prod.exe, st);
     launch_msm(a, ctx->msm_threads, st);
     ctx->prof.end(st);
     CKL();
     if (full && ctx->fused_fft) {
         FusedPlan p{};
         unsigned widest = 0;
-        prod = 0;
+        prod = Work();
         for (int k = 0; k < nseg; k++) {
             const int log_m = sg[k].log_m, m = 1 << log_m, G = (int)((sg[k].rows + 31) / 32);
             p.seg[k] = FusedSeg{D + lay.d_off[k] / U, (unsigned *)((char *)ws.sync.p + SYNC_HDR + lay.r_off[k])};
@@ -663,7 +698,7 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
             widest += (unsigned)G * (m / 2);
             for (int s = 0; s < log_m - 1; s++)
                 prod += stage_products((int)sg[k].rows, log_m, s, 0) + stage_products((int)sg[k].rows, log_m, s + 1, 1);
-            prod += (double)sg[k].rows * (m / 2) * ADD_P;
+            prod += Work((double)sg[k].rows * (m / 2) * ADD_P);
         }
         p.blk.nseg = nseg;
         fused_blocks_build(p.blk);
@@ -679,7 +714,7 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
         const unsigned max_blocks = (widest + FFT_WARPS - 1) / FFT_WARPS;
         p.blocks = (int)std::min<unsigned>((unsigned)(ctx->sms * per_sm), max_blocks);
         CK(cudaMemsetAsync(ws.sync.p, 0, SYNC_HDR + lay.r_bytes, st));
-        ctx->prof.begin(FK20_K_FFT_FUSED, prod, st);
+        ctx->prof.begin(FK20_K_FFT_FUSED, prod.alg, prod.exe, st);
         launch_g1_fused(p, st);
         ctx->prof.end(st);
         CKL();
@@ -691,7 +726,8 @@ int run_segments(fk20_ctx *ctx, Workspace &ws, const Seg *sg, int nseg, const fr
     }
     for (int k = 0; k < nseg; k++) {
         if (proofs) {  // compressed, data-availability order (kernels_out.cu)
-            ctx->prof.begin(FK20_K_OUTPUT, (double)sg[k].rows * (1 << sg[k].log_m) * PROOF_OUT_MP * MP, st);
+            const double po = (double)sg[k].rows * (1 << sg[k].log_m) * PROOF_OUT_MP * MP;
+            ctx->prof.begin(FK20_K_OUTPUT, po, po, st);
             launch_tile_to_proofs((uint8_t *)out, D + lay.d_off[k] / U, sg[k].out_off, (int)sg[k].rows,
                                   sg[k].log_m, st);
             ctx->prof.end(st);
@@ -970,6 +1006,15 @@ int fk20_ctx_profile_read(fk20_ctx *ctx, int kind, double *ms, long *launches, d
     if (ms) *ms = ctx->prof.ms[kind];
     if (launches) *launches = ctx->prof.launches[kind];
     if (products) *products = ctx->prof.products[kind];
+    return 0;
+}
+
+int fk20_ctx_profile_read_executed(fk20_ctx *ctx, int kind, double *products) {
+    if (!ctx || kind < 0 || kind >= FK20_NKINDS || !products) return FK20_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    ctx->prof.collect();
+    *products = ctx->prof.executed[kind];
     return 0;
 }
 
@@ -1358,8 +1403,8 @@ int fk20_ctx_commit(fk20_ctx *ctx, g1p_t *commitment, const fr_t *polynomial, un
     const int G = (int)((rows + 31) / 32);
     const int parts = commit_parts((int)rows, (int)n);
     CKR(ctx->commit.part.reserve(tile_bytes(G, parts)));
-    const double prod = (double)rows * n * ctx->commit.W * MADD_P + (double)rows * parts * ADD_P;
-    ctx->prof.begin(FK20_K_MSM, prod, S_(stream));
+    const double terms = (double)rows * n * ctx->commit.W, sums = (double)rows * parts * ADD_P;
+    ctx->prof.begin(FK20_K_MSM, terms * MADD_A + sums, terms * MADD_X + sums, S_(stream));
     launch_commit((uint64_t *)commitment, (uint4 *)ctx->commit.part.p, (const uint64_t *)polynomial,
                   (const uint4 *)ctx->commit.table.p, (int)rows, (int)n, ctx->commit.W, ctx->commit.cb, S_(stream));
     ctx->prof.end(S_(stream));

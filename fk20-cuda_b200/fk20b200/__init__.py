@@ -36,7 +36,7 @@ ABI_SYMBOLS = (
     "fk20_hext_fft2h", "fk20_hext_fft2hext", "fk20_h2h_fft", "fk20_hext2h", "fk20_setup2xext_fft",
     "fr_fft", "fr_ift", "g1p_fft", "g1p_ift", "fr_fft_n", "g1p_fft_n", "fp_op_n", "fr_op_n",
     "g1p_op_n", "fr_eq_n", "g1p_eq_n", "g1a_fromG1p_n", "fk20_bench_field", "fk20_version",
-    "fk20_ctx_profile", "fk20_ctx_profile_read", "fk20_program_cost", "fk20_bench_imad",
+    "fk20_ctx_profile", "fk20_ctx_profile_read", "fk20_ctx_profile_read_executed", "fk20_program_cost", "fk20_bench_imad",
     "fk20_ctx_set", "fk20_ctx_status", "g1p_fft_noalloc", "fk20_ctx_get", "fk20_plan_create",
     "fk20_plan_launch", "fk20_plan_destroy", "fk20_ctx_autotune", "fk20_server_create", "fk20_server_submit",
     "fk20_server_wait", "fk20_server_get_stats", "fk20_server_reset_stats", "fk20_server_destroy",
@@ -148,6 +148,7 @@ def lib() -> ctypes.CDLL:
             "fk20_ctx_profile": ([vp, i], i),
             "fk20_ctx_profile_read": ([vp, i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long),
                                        ctypes.POINTER(ctypes.c_double)], i),
+            "fk20_ctx_profile_read_executed": ([vp, i, ctypes.POINTER(ctypes.c_double)], i),
             "fk20_program_cost": ([i, ctypes.POINTER(i), ctypes.POINTER(i)], i),
             "fk20_bench_imad": ([vp, i, i, i, vp], i),
             "fk20_ctx_set": ([vp, i, i], i),
@@ -313,12 +314,22 @@ class Context:
         call("fk20_ctx_profile", self.h, int(enable))
 
     def profile_read(self) -> dict:
-        """{kind: (ms, launches, products)} accumulated since profile(True)."""
+        """{kind: (ms, launches, products)} accumulated since profile(True);
+        products are algorithmic limb products (fixed unit costs)."""
         out = {}
         for k, name in enumerate(KINDS):
             ms, n, pr = ctypes.c_double(), ctypes.c_long(), ctypes.c_double()
             call("fk20_ctx_profile_read", self.h, k, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(pr))
             out[name] = (ms.value, n.value, pr.value)
+        return out
+
+    def profile_read_executed(self) -> dict:
+        """{kind: products} as executed by the kernels' formulas, same launches."""
+        out = {}
+        for k, name in enumerate(KINDS):
+            pr = ctypes.c_double()
+            call("fk20_ctx_profile_read_executed", self.h, k, ctypes.byref(pr))
+            out[name] = pr.value
         return out
 
 

@@ -176,10 +176,17 @@ size_t fk20_ctx_device_bytes(const fk20_ctx *ctx);
 /* Per-launch profiling (no reference counterpart; the reference times whole
  * calls with cudaEvents in fk20benchmark.cu:103-116).  While enabled, every
  * pipeline kernel a call on this context launches is bracketed by CUDA events
- * on its stream and tagged with its algorithmic work in 32x32->64-bit limb
- * products.  fk20_ctx_profile(ctx, 1) resets the totals and enables;
+ * on its stream and tagged with its work in 32x32->64-bit limb products.
+ * fk20_ctx_profile(ctx, 1) resets the totals and enables;
  * fk20_ctx_profile_read waits for the recorded launches and returns the totals
- * of one kernel kind. */
+ * of one kernel kind, its work counted ALGORITHMICALLY: an Fp product or
+ * square 300 limb products, an Fr product 136, a G1 addition 12, mixed
+ * addition 11 and doubling 8 Fp products, a fixed-scalar multiplication its
+ * chain's doublings and additions at those prices (the work the roofline
+ * fraction divides by, whatever formulas a kernel uses).
+ * fk20_ctx_profile_read_executed returns the same kind's work as EXECUTED by
+ * the kernels' cheaper formulas (triangular squares of 234, XYZZ mixed
+ * additions of 8 M + 2 S, Jacobian twiddle programs on an isomorphic curve). */
 #define FK20_K_TC_FFT 0    /* toeplitz + Fr FFTs */
 #define FK20_K_MSM 1       /* fixed-base MSM */
 #define FK20_K_STAGE_INV 2 /* inverse G1 FFT stages */
@@ -190,6 +197,7 @@ size_t fk20_ctx_device_bytes(const fk20_ctx *ctx);
 #define FK20_NKINDS 7
 int fk20_ctx_profile(fk20_ctx *ctx, int enable);
 int fk20_ctx_profile_read(fk20_ctx *ctx, int kind, double *ms, long *launches, double *products);
+int fk20_ctx_profile_read_executed(fk20_ctx *ctx, int kind, double *products);
 
 /* Doublings and additions of the fixed-scalar G1 program `index` (0..511:
  * w_512^index; 512 + s: 2^-s), for work accounting. */

@@ -343,6 +343,50 @@ def test_launch_shape_options_agree(engine):
         ctx.set(engine.FK20_OPT_MSM_THREADS, 96)
 
 
+def test_profile_work_accounting(engine):
+    """The profiler tags each launch with its algorithmic work -- Fp product or
+    square 300 limb products, Fr product 136, G1 addition 12, mixed addition
+    11, doubling 8 Fp products, a twiddle its chain's doublings and additions
+    plus phi -- recomputed here from the program costs; the executed work of
+    the same launches (the kernels' cheaper formulas) is below it."""
+    MP, MS_X = 300, 234
+    n, rows, window, log_m = 1024, 32, 8, 7
+    m = 1 << log_m
+    c = engine.Context(0, window)
+    c.load_xext_fft(n, engine.to_device(fk20_setup_data(n)[2]))
+    poly = engine.to_device(O.seeded_fr(77, rows * n).reshape(rows, n, 4))
+    h = engine.empty((rows, m, 18))
+    c.profile(True)
+    c.poly2h_fft(h, poly, rows, n)
+    alg, exe = c.profile_read(), c.profile_read_executed()
+    c.profile(False)
+    c.close()
+
+    def prog(t):
+        d, a = engine.program_cost(t)
+        return d * 8 * MP + a * 12 * MP + MP if (d or a) else 0
+
+    def stage(s, kind):
+        tot = 0
+        for b in range(m // 2):
+            if kind == 0:
+                j = b & ((m >> (s + 1)) - 1)
+                tix = ((m - (j << s)) << (9 - log_m)) & 511
+            else:
+                j = b & ((1 << s) - 1)
+                tix = (j << (log_m - 1 - s)) << (9 - log_m)
+            tot += 2 * 12 * MP + prog(tix)
+        return tot * rows
+
+    fft = sum(stage(s, 0) + stage(s + 1, 1) for s in range(log_m - 1)) + rows * (m // 2) * 12 * MP
+    W = -(-129 // window)  # windows per GLV half
+    assert alg["fft_fused"][1] == 1 and alg["fft_fused"][2] == pytest.approx(fft, rel=1e-12)
+    assert alg["msm"][2] == pytest.approx(rows * m * (16 * 2 * W * 11 * MP + MP), rel=1e-12)
+    assert exe["msm"] == pytest.approx(rows * m * (16 * 2 * W * (8 * MP + 2 * MS_X) + MP), rel=1e-12)
+    assert 0 < exe["fft_fused"] < 0.95 * alg["fft_fused"][2]
+    assert exe["tc_fft"] == alg["tc_fft"][2] > 0
+
+
 def test_autotune_keeps_results(engine):
     """The autotuner picks a window within the table budget and launch shapes;
     the tuned context still gives the same proofs."""
