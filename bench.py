@@ -118,7 +118,8 @@ def dist_init(args, backend: str = "nccl"):
         import torch.distributed as dist
         if backend == "nccl":
             torch.cuda.set_device(local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+            # short: a rank that never reaches a collective ends the others' wait with an error
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
                                     device_id=torch.device("cuda", local))
         else:
             dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
