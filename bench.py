@@ -477,7 +477,7 @@ def run_ours(args, ws, rank, dev):
                "output_matches_device_run": same}
 
     # ---- CPU baseline: the oracle (FK20Py restated in C) on the host cores
-    cpu = None
+    cpu = ref_gpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         import oracle as O
         cores = os.cpu_count() or 1
@@ -492,6 +492,9 @@ def run_ours(args, ws, rank, dev):
                "sample": f"{srows} of the {rows} rows ({srows * m} proofs), {dt:.1f} s, one row per thread; "
                          "C restatement of FK20Py multi (variable-base double-and-add MSM, G1 FFT by scalar "
                          "multiplication), not py_ecc"}
+        # the reference's GPU baseline: its own CUDA pipeline on the same batch
+        ref_gpu = reference_gpu_same_batch(args, E, poly, xd, h_fft)
+        del xd
 
     # ---- the rest of the metric at N = 1: the ragged batch and the served load
     ragged = served = None
@@ -517,7 +520,7 @@ def run_ours(args, ws, rank, dev):
         "config": workload_config(args, {"setup_s": round(setup_s, 2),
                                          "table_bytes": table_bytes, "autotune": tune}),
         "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-        "ragged": ragged, "served": served, "impl": "ours",
+        "reference_gpu": ref_gpu, "ragged": ragged, "served": served, "impl": "ours",
     }
     if ctx is not None:
         ctx.close()
@@ -1040,44 +1043,65 @@ def run_reference(args, ws, rank):
     }
 
 
-def reference_gpu_leg(args, xext, cores):
-    """The reference's own CUDA pipeline on this GPU, beside its CPU path: the
-    unmodified reference library (oracle/_ref/libfk20ref.so, built from its
-    sources for sm_100a by oracle/ref/Makefile) runs fk20_poly2h_fft
-    (fk20_poly2h_fft.cu:47-78; rows <= 512, l = 16, n = 4096) on the same
-    seeded batch as this benchmark's own arm, timed with CUDA events around the
-    call the way fk20benchmark.cu:103-116 times it.  Two rows of its output are
-    checked against the oracle."""
-    import numpy as np
+def _ref_gpu_lib():
+    """The unmodified reference library (oracle/_ref/libfk20ref.so, built from
+    its sources for sm_100a by oracle/ref/Makefile), or the reason it cannot run."""
     lib_path = os.path.join(ROOT, "oracle", "_ref", "libfk20ref.so")
     if not os.path.exists(lib_path):
-        return {"unavailable": "reference library not built (oracle/ref/Makefile)"}
-    if args.n != 4096 or args.rows > 512:
-        return {"unavailable": "the reference pipeline is fixed at n = 4096 and at most 512 rows"}
+        return None, "reference library not built (oracle/ref/Makefile)"
     try:
         import torch
         if not torch.cuda.is_available():
-            return {"unavailable": "no CUDA device"}
+            return None, "no CUDA device"
     except ImportError:
-        return {"unavailable": "torch not importable"}
+        return None, "torch not importable"
     import ctypes
-    import oracle as O
-    lib = ctypes.CDLL(lib_path, mode=os.RTLD_LOCAL)
-    rows, n, m = args.rows, args.n, 2 * args.n // L
-    poly = seeded_polys(1000, rows, n)
-    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
-    dpoly, dxext = dev(poly), dev(xext)
+    return ctypes.CDLL(lib_path, mode=os.RTLD_LOCAL), None
+
+
+def _ref_gpu_time(lib, dpoly, dxext, rows, steps):
+    """fk20_poly2h_fft of the reference on device buffers, timed with CUDA
+    events around the call as fk20benchmark.cu:103-116 does: one warm-up call,
+    then `steps` timed calls.  Returns (per-call ms list, output, error code)."""
+    import ctypes
+    import torch
+    m = 2 * 4096 // L
     out = torch.zeros((rows, m, 18), dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()  # the reference runs on the legacy default stream: nothing else in flight
     P = lambda t: ctypes.c_void_p(t.data_ptr())
     ms = ctypes.c_float(0)
     rc = lib.ref_fk20_time(P(out), P(dpoly), P(dxext), ctypes.c_uint(rows), ctypes.byref(ms))  # warm-up
-    steps = max(1, min(args.steps, 3))
     times = []
     for _ in range(steps):
         if rc:
             break
         rc = lib.ref_fk20_time(P(out), P(dpoly), P(dxext), ctypes.c_uint(rows), ctypes.byref(ms))
         times.append(ms.value)
+    return times, out, rc
+
+
+REF_GPU_PATH = ("reference fk20_poly2h_fft (fk20_poly2h_fft.cu:47-78), reference kernels compiled for sm_100a; "
+                "double-and-add fk20_msm, g1p_ift/g1p_fft wrappers")
+
+
+def reference_gpu_leg(args, xext, cores):
+    """The reference's own CUDA pipeline on this GPU, beside its CPU path: the
+    unmodified reference library runs fk20_poly2h_fft (rows <= 512, l = 16,
+    n = 4096) on the same seeded batch as this benchmark's own arm.  Two rows
+    of its output are checked against the oracle."""
+    import numpy as np
+    import torch
+    if args.n != 4096 or args.rows > 512:
+        return {"unavailable": "the reference pipeline is fixed at n = 4096 and at most 512 rows"}
+    lib, why = _ref_gpu_lib()
+    if lib is None:
+        return {"unavailable": why}
+    import oracle as O
+    rows = args.rows
+    poly = seeded_polys(1000, rows, args.n)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+    steps = max(1, min(args.steps, 3))
+    times, out, rc = _ref_gpu_time(lib, dev(poly), dev(xext), rows, steps)
     if rc:
         return {"unavailable": f"reference pipeline returned CUDA error {rc}"}
     h = out.cpu().numpy().view(np.uint64)
@@ -1085,10 +1109,33 @@ def reference_gpu_leg(args, xext, cores):
     exp = O.fk20_rows(poly[check], xext, L, cores)
     same = all(np.array_equal(O.g1_normalize(h[r]), e) for r, e in zip(check, exp))
     tot = sum(times)
+    return {"ms_per_step": tot / steps, "proofs_per_s": rows * (2 * args.n // L) * steps / (tot * 1e-3),
+            "steps": steps, "rows": rows, "n": args.n, "rows_checked_against_oracle": check,
+            "same_as_oracle": same, "path": REF_GPU_PATH}
+
+
+def reference_gpu_same_batch(args, E, poly, xext, h_fft):
+    """The reference's own CUDA pipeline run on the very batch this arm timed
+    (same polynomials, same xext_fft, device-resident), outside every timed
+    region, with each of its proofs compared with the engine's on the device
+    (projective equality): the GPU-to-GPU comparison beside the CPU baseline."""
+    import torch
+    if args.n != 4096 or args.rows > 512:
+        return {"unavailable": "the reference pipeline is fixed at n = 4096 and at most 512 rows"}
+    lib, why = _ref_gpu_lib()
+    if lib is None:
+        return {"unavailable": why}
+    rows = args.rows
+    steps = max(1, min(args.steps, 3))
+    times, out, rc = _ref_gpu_time(lib, poly.view(torch.int64), xext.view(torch.int64), rows, steps)
+    if rc:
+        return {"unavailable": f"reference pipeline returned CUDA error {rc}"}
+    same = gpu_eq(E, out.view(torch.uint64), h_fft)
+    tot = sum(times)
+    m = 2 * args.n // L
     return {"ms_per_step": tot / steps, "proofs_per_s": rows * m * steps / (tot * 1e-3), "steps": steps,
-            "rows": rows, "n": n, "rows_checked_against_oracle": check, "same_as_oracle": same,
-            "path": "reference fk20_poly2h_fft (fk20_poly2h_fft.cu:47-78), reference kernels compiled for sm_100a; "
-                    "double-and-add fk20_msm, g1p_ift/g1p_fft wrappers"}
+            "rows": rows, "n": args.n, "all_proofs_equal_engine": same, "proofs_compared": rows * m,
+            "path": REF_GPU_PATH}
 
 
 def main():
